@@ -1,0 +1,70 @@
+"""Seeded circuit generators for the benchmark workloads.
+
+``tfim_circuit`` draws exactly like the reference's ``generate_tfim_circuit``
+(src/utils/random_circuits.py:100-165): per Trotter layer one
+``rng.uniform(J-dJ, J+dJ, N-1)`` draw for the couplings, then one
+``rng.uniform(h-dh, h+dh, N)`` draw for the fields, then RZZ on (i, i+1) and
+RX on every qubit.  The same ``numpy.random.Generator`` therefore yields the
+same gate list as the reference.
+
+``brickwork_circuit`` is the 1D brickwork workload (the reference has no
+generator for it): per layer a Haar-random SU(2) on every qubit (a complex
+Gaussian 2x2, QR, columns phase-fixed by diag(R)/|diag(R)|, divided by
+sqrt(det)), then CZ on the pairs (i, i+1) with i = layer (mod 2), each pair
+skipped with probability 1/2.  All draws come from one generator, in that
+order.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .gates import CZGate, RXGate, RZZGate, SingleQubitGate
+
+
+def tfim_circuit(num_qubits, num_layers, J=1.0, h=3.0, dt=0.3, rng=None,
+                 disorder_strength_J=0.0, disorder_strength_h=0.0):
+    if rng is None:
+        rng = np.random.default_rng(0)
+    circuit = []
+    for _ in range(num_layers):
+        J_vals = rng.uniform(J - disorder_strength_J, J + disorder_strength_J, size=num_qubits - 1)
+        h_vals = rng.uniform(h - disorder_strength_h, h + disorder_strength_h, size=num_qubits)
+        for i in range(num_qubits - 1):
+            circuit.append(RZZGate(i, i + 1, J_vals[i] * dt))
+        for i in range(num_qubits):
+            circuit.append(RXGate(i, h_vals[i] * dt))
+    return circuit
+
+
+def haar_su2(rng) -> np.ndarray:
+    """Haar-random SU(2) from one seeded generator (QR of a complex Gaussian)."""
+    z = (rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))) / np.sqrt(2.0)
+    q, r = np.linalg.qr(z)
+    d = np.diag(r)
+    q = q * (d / np.abs(d))
+    return q / np.sqrt(np.linalg.det(q))
+
+
+def brickwork_circuit(num_qubits, depth, rng=None, p_skip=0.5):
+    if rng is None:
+        rng = np.random.default_rng(0)
+    circuit = []
+    for layer in range(depth):
+        for q in range(num_qubits):
+            circuit.append(SingleQubitGate(q, haar_su2(rng)))
+        for i in range(layer % 2, num_qubits - 1, 2):
+            if rng.random() < p_skip:
+                continue
+            circuit.append(CZGate(i, i + 1))
+    return circuit
+
+
+def config1_circuit(seed=0, num_qubits=24, num_layers=20):
+    """TFIM Trotter workload: J=1, h_i ~ U[0.5, 1.5] per layer and site, dt=0.1."""
+    return tfim_circuit(num_qubits, num_layers, J=1.0, h=1.0, dt=0.1,
+                        rng=np.random.default_rng(seed), disorder_strength_h=0.5)
+
+
+def config2_circuit(seed=0, num_qubits=40, depth=30):
+    """Brickwork workload: Haar SU(2) layers, CZ pairs skipped with p=1/2."""
+    return brickwork_circuit(num_qubits, depth, rng=np.random.default_rng(seed))
