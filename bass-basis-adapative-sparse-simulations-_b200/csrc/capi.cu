@@ -1,0 +1,408 @@
+// capi.cu -- the extern "C" entry points of libbass_b200.so (include/bass_b200.h).
+#include <stdlib.h>
+#include <string.h>
+
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "internal.h"
+
+namespace bass {
+
+// ---------------------------------------------------------------------------
+// instrumentation
+// ---------------------------------------------------------------------------
+struct ProfRec {
+  int slot;
+  cudaEvent_t a, b;
+};
+static std::atomic<long long> g_launches{0};
+static std::atomic<bool> g_prof{false};
+static std::mutex g_prof_mu;
+static std::vector<ProfRec> g_recs;
+static std::vector<cudaEvent_t> g_pool;
+
+static cudaEvent_t pool_event() {
+  if (!g_pool.empty()) {
+    cudaEvent_t e = g_pool.back();
+    g_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+bool prof_on() { return g_prof.load(std::memory_order_relaxed); }
+
+ProfScope::ProfScope(int s, cudaStream_t st) : slot(s), stream(st), start(nullptr), on(prof_on()) {
+  if (on) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    start = pool_event();
+    cudaEventRecord(start, stream);
+  }
+}
+
+ProfScope::~ProfScope() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (on && start) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    cudaEvent_t stop = pool_event();
+    cudaEventRecord(stop, stream);
+    g_recs.push_back(ProfRec{slot, start, stop});
+  }
+}
+
+const Device& device() {
+  static Device d = [] {
+    Device x{};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    x.sms = sms > 0 ? sms : 1;
+    x.grid_small = x.sms * 8;
+    x.grid_tile = x.sms * 2;
+    x.grid_tile_h = x.sms;
+    return x;
+  }();
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// workspace layout: a pure function of its size, so that every call can carve
+// it without extra arguments.  max_n bounds every op's input and output count.
+// ---------------------------------------------------------------------------
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct Layout {
+  size_t counters, hist1, hist2, sel, status, fp, red, part, partials, cand_bits, cand_key, tmp_keys,
+      tmp_amps, sort_hist, total;
+  long long max_tiles, sort_tiles;
+};
+
+static Layout layout_for(long long max_n) {
+  Layout L{};
+  L.max_tiles = max_n / kStep + 2;
+  L.sort_tiles = max_n / 2048 + 2;
+  size_t o = 0;
+  L.counters = o; o += align256(64 * 8);
+  L.hist1 = o; o += align256(kHistBins * 4);
+  L.hist2 = o; o += align256(kHistBins * 4);
+  L.sel = o; o += align256(sizeof(SelState));
+  L.status = o; o += align256((size_t)L.max_tiles * 8);
+  L.fp = o; o += align256(8 * 8);
+  L.red = o; o += align256(1024 * sizeof(i128));
+  L.part = o; o += align256((size_t)kMaxSets * (L.max_tiles + 1) * 6 * 8);
+  const long long np = (long long)kMaxSets * L.max_tiles > 1024 ? (long long)kMaxSets * L.max_tiles : 1024;
+  L.partials = o; o += align256((size_t)np * sizeof(Partial));
+  L.cand_bits = o; o += align256((size_t)max_n * 8);
+  L.cand_key = o; o += align256((size_t)max_n * 8);
+  L.tmp_keys = o; o += align256((size_t)max_n * 8);
+  L.tmp_amps = o; o += align256((size_t)max_n * 16);
+  L.sort_hist = o; o += align256((size_t)256 * L.sort_tiles * 4);
+  L.total = o;
+  return L;
+}
+
+size_t ws_bytes_for(long long max_n) { return layout_for(max_n < 1 ? 1 : max_n).total; }
+
+bool carve(void* ws, size_t ws_bytes, WsView* v) {
+  if (!ws || ((uintptr_t)ws & 255)) return false;
+  if (ws_bytes < ws_bytes_for(1)) return false;
+  long long lo = 1, hi = 1LL << 40;
+  while (lo < hi) {  // largest max_n whose layout fits
+    const long long mid = lo + (hi - lo + 1) / 2;
+    if (ws_bytes_for(mid) <= ws_bytes) lo = mid;
+    else hi = mid - 1;
+  }
+  const Layout L = layout_for(lo);
+  char* b = static_cast<char*>(ws);
+  v->counters = reinterpret_cast<unsigned int*>(b + L.counters);
+  v->hist1 = reinterpret_cast<unsigned int*>(b + L.hist1);
+  v->hist2 = reinterpret_cast<unsigned int*>(b + L.hist2);
+  v->sel = reinterpret_cast<SelState*>(b + L.sel);
+  v->status = reinterpret_cast<unsigned long long*>(b + L.status);
+  v->fp = reinterpret_cast<unsigned long long*>(b + L.fp);
+  v->red = reinterpret_cast<i128*>(b + L.red);
+  v->part = reinterpret_cast<long long*>(b + L.part);
+  v->partials = reinterpret_cast<Partial*>(b + L.partials);
+  v->cand_bits = reinterpret_cast<unsigned long long*>(b + L.cand_bits);
+  v->cand_key = reinterpret_cast<unsigned long long*>(b + L.cand_key);
+  v->tmp_keys = reinterpret_cast<uint64_t*>(b + L.tmp_keys);
+  v->tmp_amps = reinterpret_cast<double2*>(b + L.tmp_amps);
+  v->sort_hist = reinterpret_cast<unsigned int*>(b + L.sort_hist);
+  v->max_n = lo;
+  v->max_tiles = L.max_tiles;
+  v->sort_tiles = L.sort_tiles;
+  return true;
+}
+
+static int status_of(cudaError_t e) { return e == cudaSuccess ? BASS_OK : BASS_ERR_CUDA; }
+
+static void load_G(OpArgs& a, const double* g, int n) {
+  for (int i = 0; i < n; ++i) a.G[i] = make_double2(g[2 * i], g[2 * i + 1]);
+}
+
+}  // namespace bass
+
+using namespace bass;
+
+#define CHECK_WS(ws, bytes, v) \
+  WsView v;                    \
+  if (!carve(ws, bytes, &v)) return BASS_ERR_WORKSPACE;
+
+extern "C" {
+
+const char* bass_version(void) { return "bass_b200 1.0 (sm_100a)"; }
+
+size_t bass_state_bytes(void) { return sizeof(bass_state); }
+size_t bass_ctrl_bytes(void) { return sizeof(bass_ctrl); }
+size_t bass_workspace_bytes(int64_t max_in, int64_t max_out, int num_qubits) {
+  (void)num_qubits;
+  const long long m = max_in > max_out ? max_in : max_out;
+  return ws_bytes_for(m);
+}
+
+int bass_state_init(bass_state* st, uint64_t* keys, double* amps, int64_t cap, int num_qubits,
+                    uint64_t init_key, void* stream) {
+  if (!st || !keys || !amps || cap < 1 || num_qubits < 1 || num_qubits > BASS_MAX_QUBITS)
+    return BASS_ERR_ARG;
+  if (num_qubits < 64 && (init_key >> num_qubits) != 0) return BASS_ERR_ARG;
+  return status_of(run_state_init(st, keys, amps, cap, num_qubits, init_key, (cudaStream_t)stream));
+}
+
+int bass_state_import_into(bass_state* st, uint64_t* st_keys, double* st_amps, int64_t cap,
+                           const uint64_t* keys, const double* amps, int64_t n, int num_qubits,
+                           void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
+  if (!st || !st_keys || !st_amps || (n > 0 && (!keys || !amps)) || n < 0 || n > cap || num_qubits < 1 ||
+      num_qubits > BASS_MAX_QUBITS || !ctrl)
+    return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  if (n > v.max_n) return BASS_ERR_WORKSPACE;
+  return status_of(run_import(st, keys, amps, n, num_qubits, v, ctrl, (cudaStream_t)stream, st_keys,
+                              st_amps, cap));
+}
+
+int bass_state_export(const bass_state* st, uint64_t* out_keys, double* out_amps, void* ws,
+                      size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
+  if (!st || !out_keys || !out_amps || !ctrl) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  return status_of(run_export(st, out_keys, out_amps, 64, v, ctrl, (cudaStream_t)stream));
+}
+
+int bass_state_export_bits(const bass_state* st, uint64_t* out_keys, double* out_amps, int key_bits,
+                           void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
+  if (!st || !out_keys || !out_amps || !ctrl || key_bits < 1 || key_bits > 64) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  return status_of(run_export(st, out_keys, out_amps, key_bits, v, ctrl, (cudaStream_t)stream));
+}
+
+int bass_state_copy_desc(bass_state* dst, const bass_state* src, void* stream) {
+  if (!dst || !src) return BASS_ERR_ARG;
+  return status_of(run_copy_desc(dst, src, (cudaStream_t)stream));
+}
+
+int bass_state_clone(bass_state* dst, const bass_state* src, bass_ctrl* ctrl, void* stream) {
+  if (!dst || !src || !ctrl) return BASS_ERR_ARG;
+  return status_of(run_clone(dst, src, ctrl, (cudaStream_t)stream));
+}
+
+int bass_ctrl_init(bass_ctrl* ctrl, uint64_t* trace, int64_t trace_cap, double pr_tie_tol, void* stream) {
+  if (!ctrl || trace_cap < 0 || (trace_cap > 0 && !trace) || !(pr_tie_tol >= 0.0)) return BASS_ERR_ARG;
+  return status_of(run_ctrl_init(ctrl, trace, trace_cap, pr_tie_tol, (cudaStream_t)stream));
+}
+
+int bass_gate_1q(const bass_state* in, bass_state* out, const double* host_G, int q, bass_trunc tr,
+                 bass_ctrl* ctrl, void* ws, size_t ws_bytes, void* stream) {
+  if (!in || !out || in == out || !host_G || q < 0 || q >= BASS_MAX_QUBITS || !ctrl) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  cudaStream_t s = (cudaStream_t)stream;
+  OpArgs a{};
+  a.in = in; a.out = out; a.ctrl = ctrl; a.ws = v; a.q = q; a.gb = 0;
+  load_G(a, host_G, 4);
+  cudaError_t e = run_merge_op(K_GATE1, a, tr, 0, 0, s);
+  if (e == cudaSuccess && tr.trace) e = run_fingerprint(out, kSigPmin, nullptr, v, s, ctrl, 1, 1);
+  return status_of(e);
+}
+
+int bass_gate_2q(const bass_state* in, bass_state* tmp, bass_state* out, const double* host_G, int q1,
+                 int q2, bass_trunc tr, bass_ctrl* ctrl, void* ws, size_t ws_bytes, void* stream) {
+  if (!in || !tmp || !out || in == tmp || tmp == out || in == out || !host_G || q1 < 0 || q2 < 0 ||
+      q1 >= BASS_MAX_QUBITS || q2 >= BASS_MAX_QUBITS || q1 == q2 || !ctrl)
+    return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  cudaStream_t s = (cudaStream_t)stream;
+  // pass 1: bring q2 to the lowest physical bit (a pure reorder)
+  OpArgs a{};
+  a.in = in; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = q2; a.gb = 0;
+  bass_trunc none{};
+  none.k_cond = -1;
+  cudaError_t e = run_merge_op(K_PERM, a, none, 0, 0, s);
+  if (e != cudaSuccess) return status_of(e);
+  // pass 2: merge on q1 above it; groups of four are (b_q1, b_q2) in input-index order
+  OpArgs b{};
+  b.in = tmp; b.out = out; b.ctrl = ctrl; b.ws = v; b.q = q1; b.gb = 1;
+  load_G(b, host_G, 16);
+  e = run_merge_op(K_GATE2, b, tr, 0, 0, s);
+  if (e == cudaSuccess && tr.trace) e = run_fingerprint(out, kSigPmin, nullptr, v, s, ctrl, 1, 1);
+  return status_of(e);
+}
+
+int bass_phase_1q(bass_state* st, bass_state* tmp, const double* host_diag2, int q, bass_ctrl* ctrl,
+                  void* ws, size_t ws_bytes, void* stream) {
+  if (!st || !tmp || st == tmp || !host_diag2 || q < 0 || q >= BASS_MAX_QUBITS || !ctrl) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  return status_of(run_phase1q(st, tmp, host_diag2, q, ctrl, v, (cudaStream_t)stream));
+}
+
+int bass_phase_2q(bass_state* st, const double* host_diag4, int q1, int q2, bass_ctrl* ctrl, void* stream) {
+  if (!st || !host_diag4 || q1 < 0 || q2 < 0 || q1 >= BASS_MAX_QUBITS || q2 >= BASS_MAX_QUBITS || q1 == q2 ||
+      !ctrl)
+    return BASS_ERR_ARG;
+  return status_of(run_phase2q(st, host_diag4, q1, q2, ctrl, (cudaStream_t)stream));
+}
+
+int bass_topk(const bass_state* in, bass_state* out, bass_trunc tr, bass_ctrl* ctrl, void* ws,
+              size_t ws_bytes, void* stream) {
+  if (!in || !out || in == out || !ctrl) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  cudaStream_t s = (cudaStream_t)stream;
+  OpArgs a{};
+  a.in = in; a.out = out; a.ctrl = ctrl; a.ws = v; a.q = 0; a.gb = 0;
+  cudaError_t e = run_merge_op(K_IDENT, a, tr, 0, 0, s);
+  if (e == cudaSuccess && tr.trace) e = run_fingerprint(out, kSigPmin, nullptr, v, s, ctrl, 1, 1);
+  return status_of(e);
+}
+
+int bass_gather(const bass_state* in, bass_state* out, const int64_t* idx, int64_t n, bass_ctrl* ctrl,
+                void* stream) {
+  if (!in || !out || in == out || (n > 0 && !idx) || n < 0 || !ctrl) return BASS_ERR_ARG;
+  return status_of(run_gather(in, out, idx, n, ctrl, (cudaStream_t)stream));
+}
+
+int bass_lcg_choose(int64_t nnz, int64_t k, int64_t seed, int64_t* host_idx) {
+  if (nnz < 0 || k < 0 || k > nnz || (k > 0 && !host_idx)) return BASS_ERR_ARG;
+  std::vector<int64_t> perm((size_t)nnz);
+  for (int64_t i = 0; i < nnz; ++i) perm[(size_t)i] = i;
+  int64_t rng = seed;
+  for (int64_t i = 0; i < k; ++i) {
+    rng = (1103515245LL * rng + 12345LL) & 0x7FFFFFFFLL;
+    const int64_t r = i + (rng % (nnz - i));
+    const int64_t t = perm[(size_t)i];
+    perm[(size_t)i] = perm[(size_t)r];
+    perm[(size_t)r] = t;
+  }
+  memcpy(host_idx, perm.data(), (size_t)k * sizeof(int64_t));
+  return BASS_OK;
+}
+
+int bass_renorm(bass_state* st, int trace, bass_ctrl* ctrl, void* ws, size_t ws_bytes, void* stream) {
+  if (!st || !ctrl) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = zero_small(v, s);
+  if (e == cudaSuccess) e = run_renorm(st, ctrl, v, s);
+  if (e == cudaSuccess && trace) e = run_fingerprint(st, kSigPmin, nullptr, v, s, ctrl, 1, 0);
+  return status_of(e);
+}
+
+int bass_pr(const bass_state* st, bass_ctrl* ctrl, void* ws, size_t ws_bytes, void* stream) {
+  if (!st || !ctrl) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  return status_of(run_reduce(st, 1, nullptr, ctrl, v, (cudaStream_t)stream));
+}
+
+int bass_norm2(const bass_state* st, double* out, void* ws, size_t ws_bytes, void* stream) {
+  if (!st || !out) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  return status_of(run_reduce(st, 0, out, nullptr, v, (cudaStream_t)stream));
+}
+
+int bass_rdm_1q(const bass_state* st, int num_qubits, double* rho, bass_ctrl* ctrl, void* ws,
+                size_t ws_bytes, void* stream) {
+  if (!st || !rho || !ctrl || num_qubits < 1 || num_qubits > BASS_MAX_QUBITS) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  return status_of(run_rdm(st, num_qubits, rho, ctrl, v, (cudaStream_t)stream));
+}
+
+int bass_rotate_step(bass_state* cur, bass_state* tmp, const double* host_U, int j, int64_t k, int trace,
+                     bass_ctrl* ctrl, void* ws, size_t ws_bytes, void* stream) {
+  if (!cur || !tmp || cur == tmp || !host_U || j < 0 || j >= 64 || k < 0 || !ctrl) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  cudaStream_t s = (cudaStream_t)stream;
+  OpArgs a{};
+  a.in = cur; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = j; a.gb = 0;
+  load_G(a, host_U, 4);
+  bass_trunc tr{};
+  tr.k_cond = k;
+  tr.k_keep = k;
+  cudaError_t e = run_merge_op(K_ROT1, a, tr, 1, j, s);
+  if (e == cudaSuccess && trace) e = run_fingerprint(tmp, kSigPmin, nullptr, v, s, ctrl, 1, 0);
+  if (e == cudaSuccess) e = run_decide(cur, tmp, ctrl, v, j, trace, s);
+  return status_of(e);
+}
+
+int bass_fingerprint(const bass_state* st, double pmin, uint64_t* out6, void* ws, size_t ws_bytes,
+                     void* stream) {
+  if (!st || !out6) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  return status_of(run_fingerprint(st, pmin, out6, v, (cudaStream_t)stream, nullptr, 0, 0));
+}
+
+int bass_radix_sort_u64(uint64_t* keys, double* amps, int64_t n, int key_bits, void* ws, size_t ws_bytes,
+                        bass_ctrl* ctrl, void* stream) {
+  if ((n > 0 && (!keys || !amps)) || n < 0 || key_bits < 1 || key_bits > 64) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  if (n > v.max_n) return BASS_ERR_WORKSPACE;
+  return status_of(run_radix_sort(keys, reinterpret_cast<double2*>(amps), n, nullptr, key_bits, v, ctrl,
+                                  (cudaStream_t)stream));
+}
+
+int bass_merge_sorted(uint64_t* keys, double* amps, int64_t n, int64_t* n_out, void* ws, size_t ws_bytes,
+                      bass_ctrl* ctrl, void* stream) {
+  if ((n > 0 && (!keys || !amps)) || n < 0 || !n_out || !ctrl) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  if (n > v.max_n) return BASS_ERR_WORKSPACE;
+  return status_of(run_merge_sorted(keys, amps, n, reinterpret_cast<long long*>(n_out), v, ctrl,
+                                    (cudaStream_t)stream));
+}
+
+int64_t bass_launch_count(void) { return (int64_t)g_launches.load(); }
+
+void bass_profile_enable(int on) { g_prof.store(on != 0); }
+
+int bass_profile_collect(double* host_ms, int64_t* host_launches, int nslots) {
+  if (nslots < 0 || (nslots > 0 && (!host_ms || !host_launches))) return BASS_ERR_ARG;
+  for (int i = 0; i < nslots; ++i) { host_ms[i] = 0.0; host_launches[i] = 0; }
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (const ProfRec& r : g_recs) {
+    if (cudaEventSynchronize(r.b) != cudaSuccess) return BASS_ERR_CUDA;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    if (r.slot >= 0 && r.slot < nslots) {
+      host_ms[r.slot] += ms;
+      host_launches[r.slot] += 1;
+    }
+    g_pool.push_back(r.a);
+    g_pool.push_back(r.b);
+  }
+  g_recs.clear();
+  return BASS_OK;
+}
+
+int bass_error(bass_ctrl* ctrl, void* stream) {
+  if (!ctrl) return -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return 1 << BASS_ERR_CUDA;
+  int32_t err = 0;
+  if (cudaMemcpy(&err, &ctrl->error, sizeof err, cudaMemcpyDeviceToHost) != cudaSuccess) return 1 << BASS_ERR_CUDA;
+  if (err) {
+    const int32_t zero = 0;
+    cudaMemcpy(&ctrl->error, &zero, sizeof zero, cudaMemcpyHostToDevice);
+  }
+  return err;
+}
+
+}  // extern "C"

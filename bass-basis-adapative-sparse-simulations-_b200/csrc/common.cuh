@@ -1,0 +1,308 @@
+// common.cuh -- shared device code of libbass_b200 (sm_100a).
+//
+// Arithmetic rules (shared with the CPU oracle, so that both agree bit for bit):
+//   * complex products and sums are evaluated with explicit round-to-nearest
+//     intrinsics, never fused into FMA;
+//   * |a|^2 = re*re + im*im;
+//   * every reduction is exact and order independent: a term is truncated
+//     toward zero to a multiple of 2^-96, summed in signed 128-bit integers,
+//     and the total is rounded once to double (round to nearest even).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/bass_b200.h"
+
+namespace bass {
+
+typedef __int128 i128;
+typedef unsigned __int128 u128;
+
+constexpr int kTile = 2048;          // entries a tile CTA holds (kThreads x kPerThread)
+constexpr int kThreads = 256;        // threads per tile CTA
+constexpr int kPerThread = kTile / kThreads;
+// Merge tiles start every kStep Z positions; backing a boundary off to the
+// start of its group (at most 4 entries for 2-qubit groups) can grow a tile to
+// kStep + 4 <= kTile entries, so every entry has a thread.
+constexpr int kStep = kTile - 8;
+constexpr int kTilePad = kTile + 8;
+constexpr int kHistBins = 8192;      // 13-bit radix-select digits
+constexpr int kCandSmem = 4096;      // candidates sorted in shared memory
+constexpr int kMaxSets = 64;         // partition sets (one per qubit for RDMs)
+constexpr int kFxFrac = 96;
+constexpr long long kSpinLimit = 1LL << 22;  // a few seconds at most
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void set_error(bass_ctrl* c, int code) {
+  atomicOr(&c->error, 1 << code);
+}
+
+// ---------------------------------------------------------------------------
+// exact accumulation
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ i128 fx_from(double v) {
+  uint64_t b;
+#ifdef __CUDA_ARCH__
+  b = (uint64_t)__double_as_longlong(v);
+#else
+  memcpy(&b, &v, sizeof b);
+#endif
+  int e = (int)((b >> 52) & 0x7FF);
+  if (e == 0) return 0;
+  uint64_t m = (b & 0xFFFFFFFFFFFFFULL) | 0x10000000000000ULL;
+  int sh = e - 1075 + kFxFrac;
+  i128 r;
+  if (sh >= 0) r = (i128)((u128)m << sh);
+  else if (sh > -64) r = (i128)(m >> (-sh));
+  else r = 0;
+  return (b >> 63) ? -r : r;
+}
+
+__device__ __forceinline__ int clz128(u128 u) {
+  uint64_t hi = (uint64_t)(u >> 64), lo = (uint64_t)u;
+  return hi ? __clzll((long long)hi) : 64 + __clzll((long long)lo);
+}
+
+__device__ __forceinline__ double fx_to(i128 s) {
+  if (s == 0) return 0.0;
+  bool neg = s < 0;
+  u128 u = neg ? (u128)0 - (u128)s : (u128)s;
+  int msb = 127 - clz128(u);
+  double r;
+  if (msb <= 52) {
+    r = ldexp((double)(uint64_t)u, -kFxFrac);
+  } else {
+    int sh = msb - 52;
+    u128 mant = u >> sh;
+    u128 rem = u & (((u128)1 << sh) - 1);
+    u128 half = (u128)1 << (sh - 1);
+    if (rem > half || (rem == half && (mant & 1))) mant += 1;
+    r = ldexp((double)(uint64_t)mant, sh - kFxFrac);
+  }
+  return neg ? -r : r;
+}
+
+__device__ __forceinline__ i128 shfl_down_i128(i128 v, int off) {
+  uint64_t lo = (uint64_t)v, hi = (uint64_t)((u128)v >> 64);
+  lo = __shfl_down_sync(0xffffffffu, lo, off);
+  hi = __shfl_down_sync(0xffffffffu, hi, off);
+  return (i128)(((u128)hi << 64) | lo);
+}
+
+__device__ __forceinline__ i128 warp_sum_i128(i128 v) {
+  for (int off = 16; off > 0; off >>= 1) v += shfl_down_i128(v, off);
+  return v;  // valid in lane 0
+}
+
+// Block-wide sum of NV 128-bit values; the result is valid in thread 0.
+// scratch: NV * (blockDim/32) i128 in shared memory.
+template <int NV>
+__device__ __forceinline__ void block_sum_i128(i128 (&v)[NV], i128* scratch) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = warp_sum_i128(v[k]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) scratch[k * nw + w] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      i128 s = 0;
+      for (int i = 0; i < nw; ++i) s += scratch[k * nw + i];
+      v[k] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// complex arithmetic without fused multiply-add
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                      __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ double prob(double2 a) {
+  return __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
+}
+__device__ __forceinline__ bool cnz(double2 a) { return a.x != 0.0 || a.y != 0.0; }
+// the stored amplitude times the pending renormalisation factors
+__device__ __forceinline__ double2 scale_load(double2 a, double r0, double r1) {
+  a = make_double2(__dmul_rn(a.x, r0), __dmul_rn(a.y, r0));
+  return make_double2(__dmul_rn(a.x, r1), __dmul_rn(a.y, r1));
+}
+
+// ---------------------------------------------------------------------------
+// keys
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint64_t fmix64(uint64_t z) {
+  z ^= z >> 33; z *= 0xff51afd7ed558ccdULL;
+  z ^= z >> 33; z *= 0xc4ceb9fe1a85ec53ULL;
+  z ^= z >> 33; return z;
+}
+constexpr uint64_t kFpSalt = 0x5851F42D4C957F2DULL;
+
+// physical key -> true key, given qat[p] = qubit at physical bit p
+__device__ __forceinline__ uint64_t true_key(uint64_t y, const int8_t* qat, int nq) {
+  uint64_t x = 0;
+  while (y) {
+    int p = __ffsll((long long)y) - 1;
+    x |= 1ULL << qat[p];
+    y &= y - 1;
+  }
+  (void)nq;
+  return x;
+}
+// true key -> physical key, given pos[q]
+__device__ __forceinline__ uint64_t phys_key(uint64_t x, const int8_t* pos) {
+  uint64_t y = 0;
+  while (x) {
+    int q = __ffsll((long long)x) - 1;
+    y |= 1ULL << pos[q];
+    x &= x - 1;
+  }
+  return y;
+}
+
+// Move physical bit t down to bit position gb (bits gb..t-1 shift up by one).
+// For gb = 0 this is "target to the lowest bit"; for gb = 1 bit 0 stays.
+__device__ __forceinline__ uint64_t zmove(uint64_t y, int t, int gb) {
+  uint64_t lomask = (1ULL << gb) - 1;
+  uint64_t bt = (y >> t) & 1ULL;
+  uint64_t hi = (t >= 63) ? 0 : (y >> (t + 1)) << (t + 1);
+  uint64_t midm = ((1ULL << t) - 1) & ~lomask;  // bits gb..t-1
+  uint64_t mid = y & midm;
+  return hi | (mid << 1) | (bt << gb) | (y & lomask);
+}
+
+// ---------------------------------------------------------------------------
+// warp-cooperative searches (32 probes per step)
+// ---------------------------------------------------------------------------
+// first index in [lo, hi) where the monotone (true...false) predicate is false
+template <class Pred>
+__device__ __forceinline__ long long warp_first_false(long long lo, long long hi, Pred pred) {
+  const int lane = threadIdx.x & 31;
+  while (hi - lo > 32) {
+    long long span = hi - lo;
+    long long p = lo + (span * (lane + 1)) / 33;
+    bool t = pred(p);
+    unsigned m = __ballot_sync(0xffffffffu, t);
+    int c = __popc(m);
+    long long nlo = (c == 0) ? lo : lo + (span * c) / 33 + 1;
+    long long nhi = (c == 32) ? hi : lo + (span * (c + 1)) / 33;
+    lo = nlo;
+    hi = nhi;
+  }
+  long long p = lo + lane;
+  bool t = (p < hi) && pred(p);
+  unsigned m = __ballot_sync(0xffffffffu, t);
+  return lo + __popc(m);
+}
+
+// ---------------------------------------------------------------------------
+// decoupled look-back (exclusive prefix of per-tile counts)
+// status word: bits 62-63 flag (1 aggregate, 2 inclusive), bits 0-61 value
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kFlagAgg = 1ULL << 62;
+constexpr unsigned long long kFlagInc = 2ULL << 62;
+constexpr unsigned long long kValMask = (1ULL << 62) - 1;
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Called by one thread.  Returns the exclusive prefix of tile `tile`.
+__device__ __forceinline__ long long lookback(unsigned long long* status, long long tile,
+                                              long long agg, bass_ctrl* ctrl) {
+  if (tile == 0) {
+    st_release(&status[0], kFlagInc | (unsigned long long)agg);
+    return 0;
+  }
+  st_release(&status[tile], kFlagAgg | (unsigned long long)agg);
+  long long excl = 0;
+  long long k = tile - 1;
+  long long spins = 0;
+  while (true) {
+    unsigned long long s = ld_acquire(&status[k]);
+    if ((s >> 62) == 0) {
+      if (++spins > kSpinLimit) {
+        set_error(ctrl, BASS_ERR_WAIT);
+        break;
+      }
+      continue;
+    }
+    excl += (long long)(s & kValMask);
+    if ((s >> 62) == 2) break;
+    if (k == 0) break;
+    --k;
+  }
+  st_release(&status[tile], kFlagInc | (unsigned long long)(excl + agg));
+  return excl;
+}
+
+// ---------------------------------------------------------------------------
+// workspace
+// ---------------------------------------------------------------------------
+// tiles of an op: merge kinds step by kStep, the plain (K_IDENT) kind by kTile
+__host__ __device__ __forceinline__ long long merge_tiles(long long n) { return (n + kStep - 1) / kStep; }
+__host__ __device__ __forceinline__ long long plain_tiles(long long n) { return (n + kTile - 1) / kTile; }
+
+struct Partial {
+  i128 s[4];
+  long long c[2];
+  long long pad[2];
+};
+
+struct SelState {
+  long long n_out;       // children produced by the op (after drop rules)
+  long long k_keep;
+  long long need;        // entries still to take from the boundary bin
+  long long n_cand;
+  unsigned long long prefix;
+  unsigned long long t_bits;
+  unsigned long long t_key;
+  int do_trunc;
+  int stage;             // 0 keep all, 1 level-1 bin known, 2 level-2 bin known, 3 resolved
+  int cand_overflow;
+  int pad;
+  double total;          // exact sum of |a|^2 over the op's output
+  long long n_written;
+  double kept;
+  double kept_p2;
+};
+
+struct WsView {
+  long long* part;               // kMaxSets x (max_tiles + 1) x 6
+  unsigned long long* status;    // max_tiles
+  unsigned int* hist1;           // kHistBins
+  unsigned int* hist2;           // kHistBins
+  Partial* partials;             // kMaxSets x max_tiles
+  unsigned long long* cand_bits; // max_n
+  unsigned long long* cand_key;  // max_n
+  SelState* sel;
+  unsigned int* counters;        // 64 tile counters
+  uint64_t* tmp_keys;            // max_n
+  double2* tmp_amps;             // max_n
+  unsigned int* sort_hist;       // radix-sort tile histograms (256 x max_tiles)
+  i128* red;                     // 1024 per-CTA reduction partials
+  unsigned long long* fp;        // 8 fingerprint accumulators
+  long long max_n;
+  long long max_tiles;
+  long long sort_tiles;
+};
+
+}  // namespace bass

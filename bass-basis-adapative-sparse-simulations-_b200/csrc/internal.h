@@ -1,0 +1,105 @@
+// internal.h -- host-side launchers shared by the .cu files of libbass_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace bass {
+
+enum Kind { K_GATE1 = 0, K_ROT1 = 1, K_GATE2 = 2, K_PERM = 3, K_IDENT = 4, K_RDM = 5 };
+enum Pass { P_HIST = 0, P_HIST2 = 1, P_GATHER = 2, P_WRITE = 3, P_RDM = 4 };
+
+// Op description passed by value to every tile kernel.
+struct OpArgs {
+  const bass_state* in;
+  bass_state* out;
+  bass_ctrl* ctrl;
+  WsView ws;
+  double2 G[16];
+  int q;          // qubit whose physical bit is the merge target (K_RDM: first set)
+  int gb;         // pregrouped low bits (0, or 1 for the second pass of a 2-qubit gate)
+  int nsets;      // K_RDM: number of qubits; otherwise 1
+  int counter;    // tile-counter slot
+  int drop_zero;  // K_IDENT: drop entries whose amplitude is exactly zero
+  int guard;      // K_IDENT: run only if ws.sel->pad (zero flag) is set
+  int prof;       // count entries into ctrl->prof_in / prof_out
+  long long k_cond, k_keep;
+};
+
+enum Slot {
+  S_PARTITION = 30, S_SELECT1 = 31, S_SELECT2 = 32, S_SELECT_EXACT = 33, S_FINALIZE = 34, S_REDUCE = 35,
+  S_FINGERPRINT = 36, S_PHASE2Q = 37, S_PHASE1Q = 38, S_RDM_FINAL = 39, S_SORT = 40, S_MERGE_RUNS = 41,
+  S_SMALL = 42
+};
+
+// Brackets one kernel launch: counts it and, when profiling is on, records
+// CUDA events around it on its stream.
+struct ProfScope {
+  ProfScope(int slot, cudaStream_t s);
+  ~ProfScope();
+  int slot;
+  cudaStream_t stream;
+  cudaEvent_t start;
+  bool on;
+};
+bool prof_on();
+#define KLAUNCH(slot, stream, ...)        \
+  do {                                    \
+    ::bass::ProfScope _ps((slot), (stream)); \
+    __VA_ARGS__;                          \
+  } while (0)
+
+struct Device {
+  int sms;
+  int grid_tile;    // persistent grid of the tile kernels
+  int grid_tile_h;  // ... of the histogram passes (more shared memory)
+  int grid_small;
+};
+const Device& device();
+
+bool carve(void* ws, size_t ws_bytes, WsView* v);
+size_t ws_bytes_for(long long max_n);
+
+// merge.cu
+cudaError_t run_merge_op(int kind, OpArgs a, const bass_trunc& tr, int finalize_mode, int j,
+                         cudaStream_t s);
+cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
+                    cudaStream_t s);
+cudaError_t zero_small(const WsView& ws, cudaStream_t s);
+cudaError_t run_ident_write(OpArgs a, cudaStream_t s);
+
+// misc.cu
+cudaError_t run_reduce(const bass_state* st, int mode, double* dest, bass_ctrl* ctrl,
+                       const WsView& ws, cudaStream_t s);
+cudaError_t run_fingerprint(const bass_state* st, double pmin, uint64_t* out6, const WsView& ws,
+                            cudaStream_t s, bass_ctrl* ctrl, int append_event, int only_if_trunc);
+cudaError_t run_radix_sort(uint64_t* keys, double2* amps, long long n, const long long* n_dev,
+                           int key_bits, const WsView& ws, bass_ctrl* ctrl, cudaStream_t s);
+cudaError_t run_renorm(bass_state* st, bass_ctrl* ctrl, const WsView& ws, cudaStream_t s);
+cudaError_t run_decide(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const WsView& ws, int j,
+                       int trace, cudaStream_t s);
+cudaError_t run_phase2q(bass_state* st, const double* d, int q1, int q2, bass_ctrl* ctrl, cudaStream_t s);
+cudaError_t run_phase1q(bass_state* st, bass_state* tmp, const double* g, int q, bass_ctrl* ctrl,
+                        const WsView& ws, cudaStream_t s);
+cudaError_t run_state_init(bass_state* st, uint64_t* keys, double* amps, long long cap, int nq,
+                           uint64_t key, cudaStream_t s);
+cudaError_t run_import(bass_state* st, const uint64_t* keys, const double* amps, long long n, int nq,
+                       const WsView& ws, bass_ctrl* ctrl, cudaStream_t s, uint64_t* st_keys,
+                       double* st_amps, long long cap);
+cudaError_t run_export(const bass_state* st, uint64_t* ok, double* oa, int key_bits, const WsView& ws,
+                       bass_ctrl* ctrl, cudaStream_t s);
+cudaError_t run_merge_sorted(uint64_t* keys, double* amps, long long n, long long* n_out,
+                             const WsView& ws, bass_ctrl* ctrl, cudaStream_t s);
+cudaError_t run_clone(bass_state* dst, const bass_state* src, bass_ctrl* ctrl, cudaStream_t s);
+cudaError_t run_copy_desc(bass_state* dst, const bass_state* src, cudaStream_t s);
+cudaError_t run_gather(const bass_state* in, bass_state* out, const int64_t* idx, long long n,
+                       bass_ctrl* ctrl, cudaStream_t s);
+cudaError_t run_ctrl_init(bass_ctrl* c, uint64_t* trace, long long cap, double tol, cudaStream_t s);
+
+constexpr double kSigPmin = 1e-24;  // |a|^2 threshold of the significant-key fingerprint
+
+constexpr int kSmallWords = 64 /*counters*/ + 2 * kHistBins;  // zeroed at the start of every op
+
+}  // namespace bass

@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark of the BASS sparse-state hot path on B200.
+
+Workload (one step): ``BASS(40, 2**22).simulate(circuit)`` with default
+BASS settings on the 1D brickwork circuit of 40 qubits and depth 30 (a
+Haar-random SU(2) on every qubit each layer, CZ on alternating neighbour
+pairs each skipped with probability 1/2; seeded synthetic circuit), complex128
+amplitudes, uint64 keys, top-k budget K = 2^22.  Metric: amplitude updates per
+second (one amplitude update = one input entry transformed by one gate or one
+basis-rotation step; counted on the device).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one process per GPU (torchrun), each an independent replica of the
+workload (the path does not shard); value = sum of all ranks' updates / the
+slowest rank's time.  ``--impl reference`` times the CPU oracle (a plain-C
+restatement of the reference's Numba kernels driven like the reference) on a
+bounded sample of the same workload: the first 28 gates at K = 2^22.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "bass-basis-adapative-sparse-simulations-_b200")
+CPU_SAMPLE_GATES = 28
+
+
+def load_pkg():
+    if "bass_b200" in sys.modules:
+        return sys.modules["bass_b200"]
+    spec = importlib.util.spec_from_file_location("bass_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["bass_b200"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def args_parser():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=40)
+    ap.add_argument("--depth", type=int, default=30)
+    ap.add_argument("--k", type=int, default=2 ** 22)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-profile", action="store_true")
+    return ap
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle port of the reference's algorithm)
+# ---------------------------------------------------------------------------
+def cpu_sample(circuit, n, k):
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    oracle.build()
+    b = oracle.OracleBASS(n, k)
+    t0 = time.perf_counter()
+    b.simulate(circuit[:CPU_SAMPLE_GATES])
+    dt = time.perf_counter() - t0
+    return b.stats["amp_updates"], dt
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    pkg = load_pkg()
+    circ = pkg.circuits.config2_circuit(seed=a.seed, num_qubits=a.n, depth=a.depth)
+    for _ in range(a.warmup):
+        cpu_sample(circ, a.n, a.k)
+    ups, secs = [], []
+    for _ in range(a.steps):
+        u, dt = cpu_sample(circ, a.n, a.k)
+        ups.append(u)
+        secs.append(dt)
+    value = sum(ups) / sum(secs)
+    sample = f"first {CPU_SAMPLE_GATES} gates of the workload circuit at K={a.k}, per step"
+    line = {
+        "impl": "reference", "metric": "amp_updates_per_s", "value": value, "unit": "amp-updates/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+        "data": "synthetic (seeded brickwork circuit)",
+        "config": workload_config(a),
+        "cpu_baseline": {"value": value, "unit": "amp-updates/s", "cores": 1, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "amp-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(a):
+    return {"workload": f"BASS brickwork n={a.n} depth={a.depth} K=2^{a.k.bit_length() - 1} complex128",
+            "n_qubits": a.n, "depth": a.depth, "K": a.k, "optimize_every": 5, "buffer_factor": 2,
+            "parallelism": f"replicas x{a.gpus}", "l2": "flushed between steps (512 MB write)"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(a, rank, world, dist):
+    import numpy as np
+    import torch
+    pkg = load_pkg()
+    from bass_b200 import _native
+    from bass_b200.bass import BASS
+    _native.build()
+    L = _native.lib()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    circ = pkg.circuits.config2_circuit(seed=a.seed, num_qubits=a.n, depth=a.depth)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def step():
+        b = BASS(a.n, a.k)
+        st = b.simulate(circ)
+        return b, st
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    launches0 = L.bass_launch_count()
+    times, ups = [], []
+    for _ in range(a.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b, st = step()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+        ups.append(b.stats["amp_updates"])
+    launches = (L.bass_launch_count() - launches0) // max(a.steps, 1)
+    clocks = sampler.stop()
+    t_total = sum(times)
+    if dist is not None:
+        tt = torch.tensor([t_total], dtype=torch.float64, device=dev)
+        uu = torch.tensor([float(sum(ups))], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.all_reduce(uu, op=dist.ReduceOp.SUM)
+        t_total, u_total = float(tt.item()), float(uu.item())
+    else:
+        u_total = float(sum(ups))
+    value = u_total / t_total
+
+    # end to end through the public API: host circuit in, host state (x, alpha) out
+    e2e_t, e2e_u, h2d, d2h = [], [], 0, 0
+    for _ in range(a.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        b = BASS(a.n, a.k)
+        st = b.simulate(circ)
+        x, al = st.x, st.alpha
+        t1 = time.perf_counter()
+        e2e_t.append(t1 - t0)
+        e2e_u.append(b.stats["amp_updates"])
+        h2d = sum(g.matrix.nbytes for g in circ)
+        d2h = x.nbytes + al.nbytes
+    e2e_total = sum(e2e_t)
+    if dist is not None:
+        tt = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+        uu = torch.tensor([float(sum(e2e_u))], dtype=torch.float64, device=dev)
+        dist.all_reduce(uu, op=dist.ReduceOp.SUM)
+        e2e_value = float(uu.item()) / e2e_total
+    else:
+        e2e_value = sum(e2e_u) / e2e_total
+
+    roofline = None
+    kernels = None
+    if not a.no_profile:
+        roofline, kernels = profile_step(a, circ, L, _native, BASS, torch)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        u, dt = cpu_sample(circ, a.n, a.k)
+        cpu = {"value": u / dt, "unit": "amp-updates/s", "cores": 1, "kind": "port",
+               "sample": f"first {CPU_SAMPLE_GATES} gates of the workload circuit at K={a.k} "
+                         f"({dt:.1f} s, {u} updates)"}
+
+    if rank == 0:
+        line = {
+            "metric": "amp_updates_per_s", "value": value, "unit": "amp-updates/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t_total / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "data": "synthetic (seeded brickwork circuit)", "config": workload_config(a),
+            "e2e": {"value": e2e_value, "unit": "amp-updates/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
+            "amp_updates_per_step": int(statistics.mean(ups)), "kernels": kernels,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def profile_step(a, circ, L, nat, BASS, torch):
+    """One extra step with per-launch CUDA events and per-kernel entry counters."""
+    import numpy as np
+    L.bass_profile_enable(1)
+    ms = np.zeros(nat.PROF_SLOTS)
+    cnt = np.zeros(nat.PROF_SLOTS, dtype=np.int64)
+    L.bass_profile_collect(nat._host(ms), nat._host(cnt), nat.PROF_SLOTS)
+    b = BASS(a.n, a.k)
+    st = b.simulate(circ)
+    torch.cuda.synchronize()
+    c = st._eng.read_ctrl()
+    L.bass_profile_collect(nat._host(ms), nat._host(cnt), nat.PROF_SLOTS)
+    L.bass_profile_enable(0)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    kernels = []
+    for s in np.argsort(-ms):
+        if ms[s] <= 0:
+            break
+        nbytes = 24 * (int(c["prof_in"][s]) + int(c["prof_out"][s]))
+        kernels.append({"kernel": nat.SLOT_NAMES[s], "ms": round(float(ms[s]), 3), "launches": int(cnt[s]),
+                        "share": round(float(ms[s] / ms.sum()), 4),
+                        "gbs": round(nbytes / (ms[s] * 1e-3) / 1e9, 1) if nbytes else None})
+    tile_slots = [s for s in range(30) if ms[s] > 0]
+    dom = max(tile_slots, key=lambda s: ms[s])
+    per_launch_bytes = 24 * (int(c["prof_in"][dom]) + int(c["prof_out"][dom])) / cnt[dom]
+    avg_s = ms[dom] * 1e-3 / cnt[dom]
+    achieved = per_launch_bytes / avg_s / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic_per_entry.json")
+    if os.path.exists(tfile):
+        tj = json.load(open(tfile))
+        if nat.SLOT_NAMES[dom] in tj:
+            traffic = tj[nat.SLOT_NAMES[dom]] * per_launch_bytes / 24
+    roof = {"bound": "hbm", "kernel": nat.SLOT_NAMES[dom], "achieved": round(achieved, 1), "peak": peak,
+            "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "bytes_per_launch": per_launch_bytes,
+            "note": "algorithmic bytes = 24 B per entry read + 24 B per entry written; timing from a "
+                    "profiled step (CUDA events around each launch on its stream)"}
+    return roof, kernels[:12]
+
+
+def main():
+    a = args_parser().parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    dist = None
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        run_ours(a, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
