@@ -866,4 +866,51 @@ cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, 
   return cudaGetLastError();
 }
 
+// RDM moments with a caller-prepared workspace view: the same kernels as
+// run_rdm, without clearing any workspace region (the caller clears the tile
+// counters) and with a final reduction that refuses states whose tile count
+// exceeds the view's capacity.  Used by the no-allocation entry point.
+__global__ void k_rdm_final_bounded(const bass_state* st, double* rho, WsView ws, bass_ctrl* c) {
+  __shared__ i128 sRed[4 * 8];
+  const int set = blockIdx.x;
+  const long long ntiles = merge_tiles(st->nnz);
+  if (ntiles > ws.max_tiles) {
+    if (threadIdx.x == 0) {
+      set_error(c, BASS_ERR_WORKSPACE);
+      for (int k = 0; k < 4; ++k) rho[4 * set + k] = NAN;
+    }
+    return;
+  }
+  i128 v[4] = {0, 0, 0, 0};
+  for (long long t = threadIdx.x; t < ntiles; t += blockDim.x) {
+    const Partial& p = ws.partials[(long long)set * ws.max_tiles + t];
+    v[0] += p.s[0]; v[1] += p.s[1]; v[2] += p.s[2]; v[3] += p.s[3];
+  }
+  block_sum_i128<4>(v, sRed);
+  if (threadIdx.x == 0) {
+    double* r = rho + 4 * set;
+    r[0] = fx_to(v[0]);
+    r[1] = fx_to(v[1]);
+    r[2] = fx_to(v[2]);
+    r[3] = fx_to(v[3]);
+  }
+}
+
+cudaError_t run_rdm_prepared(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
+                             cudaStream_t s) {
+  OpArgs a{};
+  a.in = st;
+  a.out = nullptr;
+  a.ctrl = ctrl;
+  a.ws = ws;
+  a.q = 0;
+  a.gb = 0;
+  a.nsets = nq;
+  KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, nq), 256, 0, s>>>(a, K_RDM));
+  cudaError_t e = launch_tile<K_RDM, P_RDM>(a, 0, s, nullptr);
+  if (e != cudaSuccess) return e;
+  KLAUNCH(S_RDM_FINAL, s, k_rdm_final_bounded<<<nq, 256, 0, s>>>(st, rho, ws, ctrl));
+  return cudaGetLastError();
+}
+
 }  // namespace bass

@@ -188,6 +188,18 @@ int bass_norm2(const bass_state* st, double* out, void* ws, size_t ws_bytes, voi
    (rho00, rho11, Re rho01, Im rho01), device doubles. */
 int bass_rdm_1q(const bass_state* st, int num_qubits, double* rho, bass_ctrl* ctrl, void* ws,
                 size_t ws_bytes, void* stream);
+/* bass_rdm_1q for callers that cannot allocate device memory (a stream being
+   captured into a CUDA graph, a host runtime that owns all device memory, an
+   embedding that may only pass the buffers it was given).  No counterpart in
+   the reference.  The scratch is a static array inside the library (about
+   4.8 MB, held on every GPU that loads the library until exit); the state may
+   hold at most 2^20 entries (max_entries is the caller's bound on st->nnz;
+   larger values return BASS_ERR_WORKSPACE).  All calls share the array, so
+   calls that may overlap on the GPU race and must be serialised.  The first
+   call on a device looks up the array's address; make it before any stream
+   capture.  Allocates nothing. */
+int bass_rdm_1q_noalloc(const bass_state* st, int64_t max_entries, int num_qubits, double* rho,
+                        bass_ctrl* ctrl, void* stream);
 /* One coordinate-descent step of bass_simulator.py:755-814: rotate qubit j of
    *cur by host_U (2x2) into *tmp (bass_simulator.py:156-199), keep the top k
    (:565-572), renormalise (:551-554), compare PR with ctrl->pr_cur and keep the
