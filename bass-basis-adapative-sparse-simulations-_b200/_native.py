@@ -42,8 +42,8 @@ KINDS = ["gate1", "rot1", "gate2", "perm", "plain", "rdm"]
 PASSES = ["hist", "hist2", "gather", "write", "rdm"]
 SLOT_NAMES = [f"k_tile<{k},{p}>" for k in KINDS for p in PASSES] + [
     "k_partition", "k_select1", "k_select2", "k_select_exact", "k_finalize", "reductions", "k_fingerprint",
-    "k_phase2q", "k_phase1q", "k_rdm_final", "radix_sort", "merge_runs", "bookkeeping"] + \
-    [f"slot{i}" for i in range(43, 48)]
+    "k_phase2q", "k_phase1q", "k_rdm_final", "radix_sort", "merge_runs", "bookkeeping", "k_slot_hist<1>",
+    "k_slot_hist<2>", "k_slot_gather"] + [f"slot{i}" for i in range(46, 48)]
 
 
 class Trunc(ctypes.Structure):
@@ -150,7 +150,7 @@ class Engine:
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         self.max_n = int(max(max_n, 16))
         self.nq = int(num_qubits)
-        self.ws_bytes = int(self.L.bass_workspace_bytes(self.max_n, self.max_n, self.nq))
+        self.ws_bytes = int(self.L.bass_workspace_bytes(self.max_n // 4, self.max_n, self.nq))
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
         self.ctrl = torch.zeros(self.L.bass_ctrl_bytes(), dtype=torch.uint8, device=self.device)
         self.trace_cap = int(trace_cap)

@@ -161,7 +161,8 @@ size_t bass_state_bytes(void) { return sizeof(bass_state); }
 size_t bass_ctrl_bytes(void) { return sizeof(bass_ctrl); }
 size_t bass_workspace_bytes(int64_t max_in, int64_t max_out, int num_qubits) {
   (void)num_qubits;
-  const long long m = max_in > max_out ? max_in : max_out;
+  // the evaluation pass of a 2-qubit gate keeps four |a|^2 slots per input entry
+  const long long m = 4 * max_in > max_out ? 4 * max_in : max_out;
   return ws_bytes_for(m);
 }
 

@@ -254,6 +254,52 @@ __device__ __forceinline__ long long lookback(unsigned long long* status, long l
   return excl;
 }
 
+// Called by all 32 lanes of one warp; returns the exclusive prefix of `tile`
+// in every lane.  Each step reads the status words of the 32 nearest
+// predecessors at once, sums their aggregates up to the nearest inclusive one
+// and stops there, so a tile walks back 32 tiles per dependent load.
+__device__ __forceinline__ long long lookback_warp(unsigned long long* status, long long tile,
+                                                   long long agg, bass_ctrl* ctrl) {
+  const int lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) st_release(&status[0], kFlagInc | (unsigned long long)agg);
+    return 0;
+  }
+  if (lane == 0) st_release(&status[tile], kFlagAgg | (unsigned long long)agg);
+  long long excl = 0;
+  long long base = tile - 1;
+  long long spins = 0;
+  bool gave_up = false;
+  while (true) {
+    const long long k = base - lane;
+    unsigned long long s;
+    do {
+      s = (k >= 0 && !gave_up) ? ld_acquire(&status[k]) : kFlagInc;
+      if (++spins > kSpinLimit) gave_up = true;
+    } while (__any_sync(0xffffffffu, (s >> 62) == 0));
+    const unsigned inc = __ballot_sync(0xffffffffu, (s >> 62) == 2);
+    const int stop = inc ? __ffs(inc) - 1 : 32;
+    long long v = (lane <= stop) ? (long long)(s & kValMask) : 0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    excl += __shfl_sync(0xffffffffu, v, 0);
+    if (inc) break;
+    base -= 32;
+  }
+  if (gave_up && lane == 0) set_error(ctrl, BASS_ERR_WAIT);
+  if (lane == 0) st_release(&status[tile], kFlagInc | (unsigned long long)(excl + agg));
+  return excl;
+}
+
+// warp-aggregated shared-memory histogram increment; every lane of the warp
+// must call it (valid = false for lanes with nothing to add)
+__device__ __forceinline__ void hist_add(unsigned int* h, unsigned bin, bool valid) {
+  const unsigned key = valid ? bin : 0xFFFFFFFFu;
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
+  const int lane = threadIdx.x & 31;
+  if (valid && (__ffs(peers) - 1) == lane) atomicAdd(&h[bin], (unsigned)__popc(peers));
+}
+
 // ---------------------------------------------------------------------------
 // workspace
 // ---------------------------------------------------------------------------
@@ -276,13 +322,17 @@ struct SelState {
   unsigned long long t_bits;
   unsigned long long t_key;
   int do_trunc;
-  int stage;             // 0 keep all, 1 level-1 bin known, 2 level-2 bin known, 3 resolved
+  int stage;             // 0 keep all, 1 level-1 bin known, 2 level-2 bin known, 3 resolved,
+                         // 4 exact tie at bits == prefix: settle by true key
   int cand_overflow;
-  int pad;
-  double total;          // exact sum of |a|^2 over the op's output
+  int pad;               // K_IDENT guard: a zero amplitude was produced
+  double total;          // exact sum of |a|^2 over the op's output (before truncation)
+  double total_p2;       // exact sum of |a|^4 over the op's output (before truncation)
   long long n_written;
   double kept;
   double kept_p2;
+  int skip_write;        // the write pass has nothing to do (rejected rotation)
+  int pad2;
 };
 
 struct WsView {

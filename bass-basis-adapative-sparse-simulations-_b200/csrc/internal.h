@@ -31,7 +31,7 @@ struct OpArgs {
 enum Slot {
   S_PARTITION = 30, S_SELECT1 = 31, S_SELECT2 = 32, S_SELECT_EXACT = 33, S_FINALIZE = 34, S_REDUCE = 35,
   S_FINGERPRINT = 36, S_PHASE2Q = 37, S_PHASE1Q = 38, S_RDM_FINAL = 39, S_SORT = 40, S_MERGE_RUNS = 41,
-  S_SMALL = 42
+  S_SMALL = 42, S_SLOT_HIST1 = 43, S_SLOT_HIST2 = 44, S_SLOT_GATHER = 45
 };
 
 // Brackets one kernel launch: counts it and, when profiling is on, records

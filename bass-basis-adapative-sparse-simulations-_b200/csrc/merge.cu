@@ -145,65 +145,72 @@ __device__ __forceinline__ int block_excl_scan(int v, int* sWarp, int* total) {
 // ---------------------------------------------------------------------------
 // groups -> children
 // ---------------------------------------------------------------------------
-// Children of the group whose first Z-ordered entry is at merged position p
-// (0 if p does not start a group).  Keys are the new physical keys.
+// entries per group / children per group of each kind
 template <int KIND>
-__device__ __forceinline__ int group_children(int p, int E, const uint64_t* sZ, const double2* sA,
-                                              const uint16_t* sM, int gb, const double2* G,
-                                              int drop_zero, uint64_t* ck, double2* ca) {
-  const uint64_t z = sZ[sM[p]];
+struct KindTraits {
+  static constexpr int kMaxChildren = (KIND == K_GATE2) ? 4 : (KIND == K_GATE1 || KIND == K_ROT1) ? 2 : 1;
+};
+
+// Children of the group whose first Z-ordered entry is at position p of the
+// Z-ordered tile.  Returns the mask of children that exist (0 if p does not
+// start a group); child o has the new physical key base | o and amplitude
+// ca[o].  Within a group, entries are in ascending local index, so the sums
+// run over the local index in ascending order.
+template <int KIND>
+__device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t* sZ, const double2* sA, int gb,
+                                                   const double2* sG, int drop_zero, uint64_t* base,
+                                                   double2* ca) {
+  constexpr int NC = KindTraits<KIND>::kMaxChildren;
+  const uint64_t z = sZ[p];
   if (KIND == K_PERM || KIND == K_IDENT) {
-    const double2 v = sA[sM[p]];
-    if (KIND == K_IDENT && drop_zero && !cnz(v)) return 0;
-    ck[0] = z;
+    const double2 v = sA[p];
+    if (KIND == K_IDENT && drop_zero && !cnz(v)) return 0u;
+    *base = z;
     ca[0] = v;
-    return 1;
+    return 1u;
   }
   const int sh = gb + 1;
   const uint64_t gid = z >> sh;
-  if (p > 0 && (sZ[sM[p - 1]] >> sh) == gid) return 0;
-  double2 av[4];
-  int present = 0;
-  for (int r = p; r < E; ++r) {
-    const uint64_t zr = sZ[sM[r]];
-    if ((zr >> sh) != gid) break;
-    const int li = (int)(zr & ((1u << sh) - 1));
-    av[li] = sA[sM[r]];
-    present |= 1 << li;
+  if (p > 0 && (sZ[p - 1] >> sh) == gid) return 0u;
+  *base = gid << sh;
+  double2 ar[NC];
+  int lr[NC];
+#pragma unroll
+  for (int r = 0; r < NC; ++r) {
+    const uint64_t zr = (p + r < E) ? sZ[p + r] : ~0ULL;
+    const bool in = (p + r < E) && (zr >> sh) == gid;
+    lr[r] = in ? (int)(zr & ((1u << sh) - 1)) : -1;
+    ar[r] = in ? sA[p + r] : make_double2(0.0, 0.0);
   }
-  int m = 0;
+  unsigned mask = 0;
   if (KIND == K_GATE1 || KIND == K_GATE2) {
-    const int nc = 1 << sh;
-    for (int o = 0; o < nc; ++o) {
+#pragma unroll
+    for (int o = 0; o < NC; ++o) {
       double2 acc = make_double2(0.0, 0.0);
       bool have = false;
-      for (int li = 0; li < nc; ++li) {
-        if (!((present >> li) & 1)) continue;
-        const double2 pr = cmul(G[o * nc + li], av[li]);
+#pragma unroll
+      for (int r = 0; r < NC; ++r) {
+        if (lr[r] < 0) continue;
+        const double2 pr = cmul(sG[o * NC + lr[r]], ar[r]);
         if (!cnz(pr)) continue;
         acc = have ? cadd(acc, pr) : pr;
         have = true;
       }
-      if (have) {
-        ck[m] = (gid << sh) | (uint64_t)o;
-        ca[m] = acc;
-        ++m;
-      }
+      ca[o] = acc;
+      if (have) mask |= 1u << o;
     }
   } else if (KIND == K_ROT1) {
-    const double2 a0 = (present & 1) ? av[0] : make_double2(0.0, 0.0);
-    const double2 a1 = (present & 2) ? av[1] : make_double2(0.0, 0.0);
+    const double2 zero = make_double2(0.0, 0.0);
+    const double2 a0 = (lr[0] == 0) ? ar[0] : zero;
+    const double2 a1 = (lr[0] == 1) ? ar[0] : (lr[1] == 1 ? ar[1] : zero);
 #pragma unroll
     for (int o = 0; o < 2; ++o) {
-      const double2 c = cadd(cmul(G[o * 2], a0), cmul(G[o * 2 + 1], a1));
-      if (hypot(c.x, c.y) > 1e-30) {
-        ck[m] = (gid << 1) | (uint64_t)o;
-        ca[m] = c;
-        ++m;
-      }
+      const double2 c = cadd(cmul(sG[o * 2], a0), cmul(sG[o * 2 + 1], a1));
+      ca[o] = c;
+      if (hypot(c.x, c.y) > 1e-30) mask |= 1u << o;
     }
   }
-  return m;
+  return mask;
 }
 
 __device__ __forceinline__ bool keep_child(uint64_t bits, uint64_t key, const SelState& S,
@@ -214,29 +221,37 @@ __device__ __forceinline__ bool keep_child(uint64_t bits, uint64_t key, const Se
   return S.t_key == ~0ULL || true_key(key, qat, 64) <= S.t_key;
 }
 
+__host__ __device__ constexpr int slots_per_entry(int kind) {
+  return kind == K_GATE2 ? 4 : (kind == K_GATE1 || kind == K_ROT1) ? 2 : 1;
+}
+
 // ---------------------------------------------------------------------------
 // the tile kernel
 // ---------------------------------------------------------------------------
+// Passes: P_HIST (evaluate every child once: its |a|^2 bits go to the slot
+// array, plus exact count / mass sums), P_GATHER (only on an exact tie at the
+// threshold: collect (bits, true key) of the tied children), P_WRITE (write
+// the kept children in order), P_RDM (per-qubit moments).
 template <int KIND, int PASS>
-__global__ void __launch_bounds__(kThreads) k_tile(OpArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint64_t* sZ = reinterpret_cast<uint64_t*>(smem);
-  double2* sA = reinterpret_cast<double2*>(sZ + kTilePad);
-  uint16_t* sIdx = reinterpret_cast<uint16_t*>(sA + kTilePad);
-  uint16_t* sM = sIdx + kTilePad;
-  unsigned int* sHist = reinterpret_cast<unsigned int*>(sM + kTilePad);
+  double2* sA = reinterpret_cast<double2*>(sZ + kTile);
+  uint16_t* sIdx = reinterpret_cast<uint16_t*>(sA + kTile);
   __shared__ Hdr H;
   __shared__ SelState S;
-  __shared__ long long sItem, sBase;
+  __shared__ long long sItem, sBase, sZstart;
   __shared__ long long sSegLo[5], sSegOff[6];
   __shared__ int sWarp[32];
   __shared__ i128 sRed[4 * (kThreads / 32)];
+  __shared__ double2 sG[16];
 
   const int tid = threadIdx.x;
+  if (tid < 16) sG[tid] = a.G[tid];
   if (tid == 0) S = *a.ws.sel;
   __syncthreads();
-  if (PASS == P_HIST2 && S.stage != 1) return;
-  if (PASS == P_GATHER && S.stage != 2) return;
+  if (PASS == P_GATHER && S.stage != 4) return;
+  if (PASS == P_WRITE && S.skip_write) return;
   if (KIND == K_IDENT && a.guard && S.pad == 0) return;
 
   if (tid == 0) {
@@ -251,18 +266,18 @@ __global__ void __launch_bounds__(kThreads) k_tile(OpArgs a) {
     H.ntiles = (KIND == K_IDENT) ? plain_tiles(H.n) : merge_tiles(H.n);
     out_order(in, KIND, H.t, a.gb, H.qat_out);
   }
-  if (PASS == P_HIST || PASS == P_HIST2)
-    for (int i = tid; i < kHistBins; i += kThreads) sHist[i] = 0;
   __syncthreads();
 
   const int gb = a.gb;
   const long long ntiles = H.ntiles;
-  if (ntiles > a.ws.max_tiles) {  // the workspace is too small for this state
+  constexpr int NS = slots_per_entry(KIND);
+  if (ntiles > a.ws.max_tiles || (PASS == P_HIST && (long long)NS * H.n > a.ws.max_n)) {
     if (blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
     return;
   }
+  const bool scaled = !(H.r0 == 1.0 && H.r1 == 1.0);
   const long long nitems = (KIND == K_RDM) ? ntiles * a.nsets : ntiles;
-  i128 acc[4] = {0, 0, 0, 0};
+  i128 acc[2] = {0, 0};
   long long cnt = 0;
   const int base_e = tid * kPerThread;
 
@@ -278,12 +293,15 @@ __global__ void __launch_bounds__(kThreads) k_tile(OpArgs a) {
     // ---- segments ---------------------------------------------------------
     if (tid == 0) {
       long long lo[5] = {0, 0, 0, 0, 0}, len[5] = {0, 0, 0, 0, 0};
+      long long zs;
       if (KIND == K_IDENT) {
         lo[0] = tile * kTile;
         len[0] = (H.n - lo[0] < kTile) ? H.n - lo[0] : kTile;
+        zs = lo[0];
       } else {
         const long long* rc = a.ws.part + ((long long)set * (a.ws.max_tiles + 1) + tile) * 6;
         const long long* rn = rc + 6;
+        zs = rc[0];
         if (rc[1] == rn[1]) {
           lo[0] = rc[1] + rc[4]; len[0] = rn[4] - rc[4];
           lo[1] = rc[2] + rc[5]; len[1] = rn[5] - rc[5];
@@ -303,46 +321,82 @@ __global__ void __launch_bounds__(kThreads) k_tile(OpArgs a) {
         sSegOff[k] = o;
         o += len[k];
       }
-      if (o > kTile || bad) {  // inconsistent partition: skip the tile, report
+      if (o > kTile || bad || zs < 0 || zs + o > H.n) {  // inconsistent partition: skip the tile, report
         set_error(a.ctrl, BASS_ERR_ARG);
         for (int k = 0; k < 5; ++k) sSegOff[k] = 0;
         o = 0;
       }
       sSegOff[5] = o;
+      sZstart = zs;
       if (a.prof) atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_in[KIND * 5 + PASS]),
                             (unsigned long long)o);
     }
     __syncthreads();
     const int E = (int)sSegOff[5];
 
-    // ---- load (Z keys, scaled amplitudes) ---------------------------------
-    for (int e = tid; e < E; e += kThreads) {
-      int k = 0;
-      while (k < 4 && e >= sSegOff[k + 1]) ++k;
-      const long long g = sSegLo[k] + (e - sSegOff[k]);
-      const uint64_t y = H.keys[g];
-      sZ[e] = (KIND == K_IDENT) ? y : zmove(y, t, gb);
-      sA[e] = scale_load(H.amps[g], H.r0, H.r1);
+    // ---- load: Z keys and amplitudes (pending renormalisation applied) -----
+    // All of a thread's loads are issued before its shared-memory stores.
+    const int o1 = (int)sSegOff[1], o2 = (int)sSegOff[2], o3 = (int)sSegOff[3], o4 = (int)sSegOff[4];
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      constexpr int L = kPerThread / 2;
+      uint64_t ry[L];
+      double2 rv[L];
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        const int e = (half * L + k) * kThreads + tid;
+        if (e < E) {
+          const int sg = (e >= o1) + (e >= o2) + (e >= o3) + (e >= o4);
+          const long long src = sSegLo[sg] + (e - sSegOff[sg]);
+          ry[k] = H.keys[src];
+          rv[k] = H.amps[src];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        const int e = (half * L + k) * kThreads + tid;
+        if (e < E) {
+          sZ[e] = (KIND == K_IDENT) ? ry[k] : zmove(ry[k], t, gb);
+          sA[e] = scaled ? scale_load(rv[k], H.r0, H.r1) : rv[k];
+        }
+      }
     }
     __syncthreads();
 
-    // ---- Z order: split by the target bit, merge ---------------------------
+    // ---- Z order: stable split by the target bit, merge, write back --------
     if (KIND != K_IDENT) {
+      const int lane = tid & 31, w = tid >> 5;
+      const unsigned lt = (1u << lane) - 1;
+      unsigned m0[kPerThread];
       int c0 = 0;
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
-        const int e = base_e + k;
-        if (e < E && !((sZ[e] >> gb) & 1ULL)) ++c0;
+        const int e = w * 256 + k * 32 + lane;
+        const bool is0 = e < E && !((sZ[e] >> gb) & 1ULL);
+        m0[k] = __ballot_sync(0xffffffffu, is0);
+        c0 += __popc(m0[k]);
       }
-      int n0;
-      const int ex0 = block_excl_scan(c0, sWarp, &n0);
-      int w0 = ex0, w1 = (base_e < E ? base_e : E) - ex0;
+      if (lane == 0) sWarp[w] = c0;
+      __syncthreads();
+      int wb0 = 0, n0 = 0;
+#pragma unroll
+      for (int i = 0; i < kThreads / 32; ++i) {
+        const int v = sWarp[i];
+        if (i < w) wb0 += v;
+        n0 += v;
+      }
+      const int wstart = w * 256 < E ? w * 256 : E;
+      int r0 = wb0, r1 = wstart - wb0;
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
-        const int e = base_e + k;
-        if (e >= E) break;
-        if (!((sZ[e] >> gb) & 1ULL)) sIdx[w0++] = (uint16_t)e;
-        else sIdx[n0 + w1++] = (uint16_t)e;
+        const int e = w * 256 + k * 32 + lane;
+        const unsigned ones = __ballot_sync(0xffffffffu, e < E) & ~m0[k];
+        if (e < E) {
+          if ((m0[k] >> lane) & 1u) sIdx[r0 + __popc(m0[k] & lt)] = (uint16_t)e;
+          else sIdx[n0 + r1 + __popc(ones & lt)] = (uint16_t)e;
+        }
+        r0 += __popc(m0[k]);
+        r1 += __popc(ones);
       }
       __syncthreads();
       const int n1 = E - n0;
@@ -356,31 +410,51 @@ __global__ void __launch_bounds__(kThreads) k_tile(OpArgs a) {
         else hi = m;
       }
       int i = lo, j = d - lo;
+      uint64_t rz[kPerThread];
+      double2 ra[kPerThread];
+      uint64_t z0 = (i < n0) ? sZ[S0[i]] : ~0ULL;
+      uint64_t z1 = (j < n1) ? sZ[S1[j]] : ~0ULL;
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
-        const int p = d + k;
-        if (p >= E) break;
-        const bool take0 = i < n0 && (j >= n1 || sZ[S0[i]] < sZ[S1[j]]);
-        sM[p] = take0 ? S0[i++] : S1[j++];
+        if (d + k < E) {
+          if (z0 < z1) {
+            rz[k] = z0;
+            ra[k] = sA[S0[i]];
+            ++i;
+            z0 = (i < n0) ? sZ[S0[i]] : ~0ULL;
+          } else {
+            rz[k] = z1;
+            ra[k] = sA[S1[j]];
+            ++j;
+            z1 = (j < n1) ? sZ[S1[j]] : ~0ULL;
+          }
+        }
       }
-    } else {
-      for (int e = tid; e < E; e += kThreads) sM[e] = (uint16_t)e;
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kPerThread; ++k) {
+        if (d + k < E) {
+          sZ[d + k] = rz[k];
+          sA[d + k] = ra[k];
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
 
     // ---- evaluate ------------------------------------------------------------
-    const int pend = (base_e + kPerThread < E) ? base_e + kPerThread : E;
+    // Round r gives position r * kThreads + tid to thread tid, so neighbouring
+    // threads handle neighbouring groups and write neighbouring outputs.
     if (PASS == P_RDM) {
       i128 v[4] = {0, 0, 0, 0};
-      for (int p = base_e; p < pend; ++p) {
-        const uint64_t z = sZ[sM[p]];
+      for (int p = tid; p < E; p += kThreads) {
+        const uint64_t z = sZ[p];
         const uint64_t gid = z >> 1;
-        if (p > 0 && (sZ[sM[p - 1]] >> 1) == gid) continue;
-        const double2 x0 = sA[sM[p]];
+        if (p > 0 && (sZ[p - 1] >> 1) == gid) continue;
+        const double2 x0 = sA[p];
         if ((z & 1ULL) == 0) {
           v[0] += fx_from(prob(x0));
-          if (p + 1 < E && (sZ[sM[p + 1]] >> 1) == gid) {
-            const double2 x1 = sA[sM[p + 1]];
+          if (p + 1 < E && (sZ[p + 1] >> 1) == gid) {
+            const double2 x1 = sA[p + 1];
             v[1] += fx_from(prob(x1));
             const double2 c = cmul(x0, make_double2(x1.x, -x1.y));
             v[2] += fx_from(c.x);
@@ -396,35 +470,65 @@ __global__ void __launch_bounds__(kThreads) k_tile(OpArgs a) {
         pt->s[0] = v[0]; pt->s[1] = v[1]; pt->s[2] = v[2]; pt->s[3] = v[3];
       }
     } else if (PASS == P_WRITE) {
-      uint64_t ck[4];
-      double2 ca[4];
-      int kc = 0;
-      for (int p = base_e; p < pend; ++p) {
-        const int m = group_children<KIND>(p, E, sZ, sA, sM, gb, a.G, a.drop_zero, ck, ca);
-        for (int c = 0; c < m; ++c)
-          if (keep_child((uint64_t)__double_as_longlong(prob(ca[c])), ck[c], S, H.qat_out)) ++kc;
-      }
-      int tile_total;
-      const int ex = block_excl_scan(kc, sWarp, &tile_total);
-      if (tid == 0) {
-        const long long b = lookback(a.ws.status, tile, tile_total, a.ctrl);
-        sBase = b;
-        if (tile == ntiles - 1) a.ws.sel->n_written = b + tile_total;
-        if (b + tile_total > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
-        if (a.prof) atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_out[KIND * 5 + PASS]),
-                              (unsigned long long)tile_total);
+      constexpr int MC = KindTraits<KIND>::kMaxChildren;
+      uint64_t kb;
+      double2 ca[MC];
+      uint16_t* sOff = sIdx;  // free after the merge
+      // (a) kept children per position
+      for (int p = tid; p < E; p += kThreads) {
+        const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+        int kc = 0;
+#pragma unroll
+        for (int c = 0; c < MC; ++c)
+          if (((cm >> c) & 1u) &&
+              keep_child((uint64_t)__double_as_longlong(prob(ca[c])), kb | (uint64_t)c, S, H.qat_out))
+            ++kc;
+        sOff[p] = (uint16_t)kc;
       }
       __syncthreads();
-      long long o = sBase + ex;
+      // (b) counts -> exclusive offsets in place (position order)
+      int run = 0;
+#pragma unroll
+      for (int k = 0; k < kPerThread; ++k)
+        if (base_e + k < E) run += sOff[base_e + k];
+      int tile_total;
+      int ex = block_excl_scan(run, sWarp, &tile_total);
+#pragma unroll
+      for (int k = 0; k < kPerThread; ++k) {
+        const int p = base_e + k;
+        if (p < E) {
+          const int c = sOff[p];
+          sOff[p] = (uint16_t)ex;
+          ex += c;
+        }
+      }
+      // (c) the tile's base in the output
+      if (tid < 32) {
+        const long long b = lookback_warp(a.ws.status, tile, tile_total, a.ctrl);
+        if (tid == 0) {
+          sBase = b;
+          if (tile == ntiles - 1) a.ws.sel->n_written = b + tile_total;
+          if (b + tile_total > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
+          if (a.prof) atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_out[KIND * 5 + PASS]),
+                                (unsigned long long)tile_total);
+        }
+      }
+      __syncthreads();
+      // (d) write the kept children
       if (sBase + tile_total <= a.out->cap) {
         uint64_t* ok = a.out->keys;
         double2* oa = reinterpret_cast<double2*>(a.out->amps);
-        for (int p = base_e; p < pend; ++p) {
-          const int m = group_children<KIND>(p, E, sZ, sA, sM, gb, a.G, a.drop_zero, ck, ca);
-          for (int c = 0; c < m; ++c) {
+        for (int p = tid; p < E; p += kThreads) {
+          const int o_end = (p + 1 < E) ? sOff[p + 1] : tile_total;
+          if (o_end == sOff[p]) continue;
+          long long o = sBase + sOff[p];
+          const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+#pragma unroll
+          for (int c = 0; c < MC; ++c) {
+            if (!((cm >> c) & 1u)) continue;
             const double pv = prob(ca[c]);
-            if (keep_child((uint64_t)__double_as_longlong(pv), ck[c], S, H.qat_out)) {
-              ok[o] = ck[c];
+            if (keep_child((uint64_t)__double_as_longlong(pv), kb | (uint64_t)c, S, H.qat_out)) {
+              ok[o] = kb | (uint64_t)c;
               oa[o] = ca[c];
               ++o;
               acc[0] += fx_from(pv);
@@ -433,30 +537,51 @@ __global__ void __launch_bounds__(kThreads) k_tile(OpArgs a) {
           }
         }
       }
-    } else {
-      uint64_t ck[4];
-      double2 ca[4];
-      for (int p = base_e; p < pend; ++p) {
-        const int m = group_children<KIND>(p, E, sZ, sA, sM, gb, a.G, a.drop_zero, ck, ca);
-        for (int c = 0; c < m; ++c) {
-          const double pv = prob(ca[c]);
-          const uint64_t bits = (uint64_t)__double_as_longlong(pv);
-          if (PASS == P_HIST) {
-            atomicAdd(&sHist[bits >> 50], 1u);
+    } else if (PASS == P_HIST) {
+      uint64_t kb;
+      double2 ca[NS];
+      unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys) + NS * sZstart;
+      for (int p = tid; p < E; p += kThreads) {
+        const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+        unsigned long long sb[NS];
+#pragma unroll
+        for (int c = 0; c < NS; ++c) {
+          if ((cm >> c) & 1u) {
+            const double pv = prob(ca[c]);
+            sb[c] = (unsigned long long)__double_as_longlong(pv);
             acc[0] += fx_from(pv);
+            acc[1] += fx_from(__dmul_rn(pv, pv));
             ++cnt;
-          } else if (PASS == P_HIST2) {
-            if ((bits >> 50) == S.prefix) atomicAdd(&sHist[(bits >> 37) & (kHistBins - 1)], 1u);
-          } else if (PASS == P_GATHER) {
-            if ((bits >> 37) == S.prefix) {
-              const unsigned long long slot =
-                  atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws.sel->n_cand), 1ULL);
-              if ((long long)slot < a.ws.max_n) {
-                a.ws.cand_bits[slot] = bits;
-                a.ws.cand_key[slot] = true_key(ck[c], H.qat_out, 64);
-              } else {
-                a.ws.sel->cand_overflow = 1;
-              }
+          } else {
+            sb[c] = ~0ULL;
+          }
+        }
+        if (NS == 1) {
+          slots[p] = sb[0];
+        } else {
+#pragma unroll
+          for (int c = 0; c < NS; c += 2)
+            *reinterpret_cast<ulonglong2*>(slots + (long long)NS * p + c) = make_ulonglong2(sb[c], sb[c + 1]);
+        }
+      }
+    } else if (PASS == P_GATHER) {
+      constexpr int MC = KindTraits<KIND>::kMaxChildren;
+      uint64_t kb;
+      double2 ca[MC];
+      for (int p = tid; p < E; p += kThreads) {
+        const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+#pragma unroll
+        for (int c = 0; c < MC; ++c) {
+          if (!((cm >> c) & 1u)) continue;
+          const uint64_t bits = (uint64_t)__double_as_longlong(prob(ca[c]));
+          if (bits == S.prefix) {
+            const unsigned long long slot =
+                atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws.sel->n_cand), 1ULL);
+            if ((long long)slot < a.ws.max_n) {
+              a.ws.cand_bits[slot] = bits;
+              a.ws.cand_key[slot] = true_key(kb | (uint64_t)c, H.qat_out, 64);
+            } else {
+              a.ws.sel->cand_overflow = 1;
             }
           }
         }
@@ -466,18 +591,88 @@ __global__ void __launch_bounds__(kThreads) k_tile(OpArgs a) {
   }
 
   // ---- flush ---------------------------------------------------------------
-  if (PASS == P_HIST || PASS == P_HIST2) {
-    unsigned int* gh = (PASS == P_HIST) ? a.ws.hist1 : a.ws.hist2;
-    for (int i = tid; i < kHistBins; i += kThreads)
-      if (sHist[i]) atomicAdd(&gh[i], sHist[i]);
-  }
   if (PASS == P_HIST || PASS == P_WRITE) {
-    i128 v[2] = {acc[0], (i128)cnt};
-    block_sum_i128<2>(v, sRed);
+    i128 v[3] = {acc[0], acc[1], (i128)cnt};
+    block_sum_i128<3>(v, sRed);
     if (tid == 0) {
       Partial* pt = a.ws.partials + blockIdx.x;
       pt->s[0] = v[0];
-      pt->c[0] = (long long)v[1];
+      pt->s[1] = v[1];
+      pt->c[0] = (long long)v[2];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// streaming passes over the slot array (one |a|^2 bit pattern per child,
+// ~0 where a group has fewer children than slots)
+// ---------------------------------------------------------------------------
+// LEVEL 1: histogram of bits >> 50 over all slots, only when the op
+// truncates (count from the evaluation pass's per-CTA partials); LEVEL 2:
+// bits 37-49 of the slots inside the level-1 boundary bin.
+template <int LEVEL>
+__global__ void __launch_bounds__(256) k_slot_hist(OpArgs a, int ns, int nblk) {
+  __shared__ unsigned int h[kHistBins];
+  __shared__ int sGo;
+  __shared__ unsigned long long sPrefix;
+  __shared__ long long sCnt[8];
+  if (LEVEL == 1) {
+    long long c = 0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) c += a.ws.partials[b].c[0];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+    if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      long long n_out = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) n_out += sCnt[w];
+      sGo = !(a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out || a.k_keep <= 0);
+      sPrefix = 0;
+    }
+  } else if (threadIdx.x == 0) {
+    sGo = a.ws.sel->stage == 1;
+    sPrefix = a.ws.sel->prefix;
+  }
+  __syncthreads();
+  if (!sGo) return;
+  for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const long long nslots = (long long)ns * a.in->nnz;
+  if (nslots > a.ws.max_n) return;
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  const unsigned long long pre = sPrefix;
+  for (long long b = (long long)blockIdx.x * blockDim.x; b < nslots; b += (long long)gridDim.x * blockDim.x) {
+    const long long i = b + threadIdx.x;
+    const unsigned long long bits = (i < nslots) ? slots[i] : ~0ULL;
+    const bool valid = bits != ~0ULL && (LEVEL == 1 || (bits >> 50) == pre);
+    const unsigned bin = LEVEL == 1 ? (unsigned)(bits >> 50) : (unsigned)((bits >> 37) & (kHistBins - 1));
+    hist_add(h, bin, valid);
+  }
+  __syncthreads();
+  unsigned int* gh = LEVEL == 1 ? a.ws.hist1 : a.ws.hist2;
+  for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
+    if (h[i]) atomicAdd(&gh[i], h[i]);
+}
+
+// candidates of the level-2 boundary bin: (bits, slot index)
+__global__ void __launch_bounds__(256) k_slot_gather(OpArgs a, int ns) {
+  SelState* sel = a.ws.sel;
+  if (sel->stage != 2) return;
+  const unsigned long long pre = sel->prefix;
+  const long long nslots = (long long)ns * a.in->nnz;
+  if (nslots > a.ws.max_n) return;
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots;
+       i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long bits = slots[i];
+    if (bits != ~0ULL && (bits >> 37) == pre) {
+      const unsigned long long k = atomicAdd(reinterpret_cast<unsigned long long*>(&sel->n_cand), 1ULL);
+      if ((long long)k < a.ws.max_n) {
+        a.ws.cand_bits[k] = bits;
+        a.ws.cand_key[k] = (unsigned long long)i;
+      } else {
+        sel->cand_overflow = 1;
+      }
     }
   }
 }
@@ -531,19 +726,21 @@ __device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, 
 
 __global__ void __launch_bounds__(1024) k_select1(OpArgs a, int nblk) {
   __shared__ long long sS[1024];
-  __shared__ i128 sRed[2 * 32];
+  __shared__ i128 sRed[3 * 32];
   SelState* sel = a.ws.sel;
-  i128 v[2] = {0, 0};
+  i128 v[3] = {0, 0, 0};
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
     v[0] += a.ws.partials[b].s[0];
-    v[1] += (i128)a.ws.partials[b].c[0];
+    v[1] += a.ws.partials[b].s[1];
+    v[2] += (i128)a.ws.partials[b].c[0];
   }
-  block_sum_i128<2>(v, sRed);
+  block_sum_i128<3>(v, sRed);
   __shared__ int sGo;
   if (threadIdx.x == 0) {
-    const long long n_out = (long long)v[1];
+    const long long n_out = (long long)v[2];
     sel->n_out = n_out;
     sel->total = fx_to(v[0]);
+    sel->total_p2 = fx_to(v[1]);
     sel->k_keep = a.k_keep;
     sGo = 0;
     if (a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out) {
@@ -605,12 +802,50 @@ __device__ __forceinline__ bool better(unsigned long long ab, unsigned long long
   return ab > bb || (ab == bb && ak < bk);
 }
 
-__global__ void __launch_bounds__(1024) k_select_exact(OpArgs a) {
+// Sorts the first m candidates by (bits desc, key asc) in shared memory
+// (m <= kCandSmem); block of 1024 threads.
+__device__ void sort_candidates(unsigned long long* sb, unsigned long long* sk, long long m, const WsView& ws,
+                                bool keys_desc_by_bits_only) {
+  (void)keys_desc_by_bits_only;
+  const int tid = threadIdx.x;
+  int P = 1;
+  while (P < m) P <<= 1;
+  for (int i = tid; i < P; i += blockDim.x) {
+    if (i < m) { sb[i] = ws.cand_bits[i]; sk[i] = ws.cand_key[i]; }
+    else { sb[i] = 0; sk[i] = ~0ULL; }
+  }
+  __syncthreads();
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = tid; i < P; i += blockDim.x) {
+        const int jx = i ^ stride;
+        if (jx > i) {
+          const bool up = (i & size) == 0;
+          const bool sw = up ? better(sb[jx], sk[jx], sb[i], sk[i]) : better(sb[i], sk[i], sb[jx], sk[jx]);
+          if (sw) {
+            unsigned long long tb = sb[i], tk = sk[i];
+            sb[i] = sb[jx]; sk[i] = sk[jx]; sb[jx] = tb; sk[jx] = tk;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// mode 0 (after the slot gather, stage 2): candidates are (bits, slot) of the
+//   level-2 boundary bin; find the need-th largest bit pattern T.  If every
+//   candidate equal to T is needed the threshold is resolved (keep bits >= T);
+//   otherwise the tie is settled by true key (stage 4: collect the tied
+//   children with their keys).
+// mode 1 (after the key pass, stage 4): candidates are (T, true key); keep the
+//   need smallest keys.
+__global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned long long* sb = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* sk = sb + kCandSmem;
   SelState* sel = a.ws.sel;
-  if (sel->stage != 2) return;
+  if (sel->stage != (mode == 0 ? 2 : 4)) return;
   long long m = sel->n_cand;
   if (sel->cand_overflow || m > a.ws.max_n) {
     if (threadIdx.x == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
@@ -618,71 +853,112 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a) {
   }
   const long long need = sel->need;
   const int tid = threadIdx.x;
+  __shared__ unsigned long long sT;
+  __shared__ long long sGt, sEq;
   if (m <= kCandSmem) {
-    int P = 1;
-    while (P < m) P <<= 1;
-    for (int i = tid; i < P; i += blockDim.x) {
-      if (i < m) { sb[i] = a.ws.cand_bits[i]; sk[i] = a.ws.cand_key[i]; }
-      else { sb[i] = 0; sk[i] = ~0ULL; }
-    }
-    __syncthreads();
-    for (int size = 2; size <= P; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int i = tid; i < P; i += blockDim.x) {
-          const int jx = i ^ stride;
-          if (jx > i) {
-            const bool up = (i & size) == 0;
-            const bool sw = up ? better(sb[jx], sk[jx], sb[i], sk[i]) : better(sb[i], sk[i], sb[jx], sk[jx]);
-            if (sw) {
-              unsigned long long tb = sb[i], tk = sk[i];
-              sb[i] = sb[jx]; sk[i] = sk[jx]; sb[jx] = tb; sk[jx] = tk;
-            }
-          }
-        }
-        __syncthreads();
-      }
-    }
+    sort_candidates(sb, sk, m, a.ws, mode == 0);
     if (tid == 0) {
       const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
-      sel->t_bits = sb[r];
-      sel->t_key = sk[r];
+      if (mode == 1) {
+        sel->t_bits = sb[r];
+        sel->t_key = sk[r];
+        sel->stage = 3;
+      } else {
+        const unsigned long long T = sb[r];
+        long long gt = 0, eq = 0;
+        for (long long i = 0; i < m; ++i) {
+          gt += sb[i] > T;
+          eq += sb[i] == T;
+        }
+        sT = T; sGt = gt; sEq = eq;
+      }
+    }
+  } else if (mode == 1) {
+    // all candidates share the bit pattern: radix select of the need-th smallest key
+    unsigned int* h = reinterpret_cast<unsigned int*>(smem);
+    __shared__ unsigned long long sKeyPre;
+    __shared__ long long sNeed;
+    if (tid == 0) { sKeyPre = 0; sNeed = need; }
+    __syncthreads();
+    for (int shift = 56; shift >= 0; shift -= 8) {
+      for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
+      __syncthreads();
+      const unsigned long long pre = sKeyPre;
+      for (long long i = tid; i < m; i += blockDim.x) {
+        const unsigned long long k = a.ws.cand_key[i];
+        if (shift == 56 || (k >> (shift + 8)) == pre) atomicAdd(&h[(unsigned)(k >> shift) & 255u], 1u);
+      }
+      __syncthreads();
+      if (tid == 0) {
+        long long below = 0;
+        int b = 0;
+        for (; b < 255; ++b) {
+          if (below + h[b] >= sNeed) break;
+          below += h[b];
+        }
+        sNeed -= below;
+        sKeyPre = (pre << 8) | (unsigned long long)b;
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      sel->t_bits = sel->prefix;
+      sel->t_key = sKeyPre;
       sel->stage = 3;
     }
     return;
-  }
-  // many candidates (ties): radix select on (low 37 bits of |a|^2, ~key), 8-bit digits
-  unsigned int* h = reinterpret_cast<unsigned int*>(smem);
-  __shared__ u128 sPrefix;
-  __shared__ long long sNeed;
-  if (tid == 0) { sPrefix = 0; sNeed = need; }
-  __syncthreads();
-  const unsigned long long m37 = (1ULL << 37) - 1;
-  for (int shift = 96; shift >= 0; shift -= 8) {
-    for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
+  } else {
+    // many candidates: radix select on the low 37 bits of the bit pattern
+    unsigned int* h = reinterpret_cast<unsigned int*>(smem);
+    __shared__ unsigned long long sLow;
+    __shared__ long long sNeed;
+    __shared__ unsigned int sLastCount;
+    if (tid == 0) { sLow = 0; sNeed = need; }
     __syncthreads();
-    const u128 pre = sPrefix;
-    for (long long i = tid; i < m; i += blockDim.x) {
-      const u128 comp = ((u128)(a.ws.cand_bits[i] & m37) << 64) | (u128)(~a.ws.cand_key[i]);
-      if ((comp >> (shift + 8)) == pre) atomicAdd(&h[(unsigned)(comp >> shift) & 255u], 1u);
-    }
-    __syncthreads();
-    if (tid == 0) {
-      long long above = 0;
-      int b = 255;
-      for (; b > 0; --b) {
-        if (above + h[b] >= sNeed) break;
-        above += h[b];
+    const unsigned long long m37 = (1ULL << 37) - 1;
+    for (int shift = 32; shift >= 0; shift -= 8) {
+      for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
+      __syncthreads();
+      const unsigned long long pre = sLow;
+      for (long long i = tid; i < m; i += blockDim.x) {
+        const unsigned long long lb = a.ws.cand_bits[i] & m37;
+        if (shift == 32 || (lb >> (shift + 8)) == pre) atomicAdd(&h[(unsigned)(lb >> shift) & 255u], 1u);
       }
-      sNeed -= above;
-      sPrefix = (pre << 8) | (u128)b;
+      __syncthreads();
+      if (tid == 0) {
+        long long above = 0;
+        int b = 255;
+        for (; b > 0; --b) {
+          if (above + h[b] >= sNeed) break;
+          above += h[b];
+        }
+        sNeed -= above;
+        sLow = (pre << 8) | (unsigned long long)b;
+        sLastCount = h[b];
+      }
+      __syncthreads();
     }
-    __syncthreads();
+    if (tid == 0) {
+      const unsigned long long T = (sel->prefix << 37) | sLow;
+      sT = T;
+      sGt = need - sNeed;
+      sEq = sLastCount;
+    }
   }
-  if (tid == 0) {
-    const u128 comp = sPrefix;
-    sel->t_bits = (sel->prefix << 37) | (uint64_t)((comp >> 64) & m37);
-    sel->t_key = ~(uint64_t)comp;
-    sel->stage = 3;
+  __syncthreads();
+  if (tid == 0 && mode == 0) {
+    const long long take = need - sGt;  // entries equal to T that are kept
+    if (take == sEq) {
+      sel->t_bits = sT;
+      sel->t_key = ~0ULL;
+      sel->stage = 3;
+    } else {
+      sel->stage = 4;
+      sel->prefix = sT;
+      sel->need = take;
+      sel->n_cand = 0;
+      sel->cand_overflow = 0;
+    }
   }
 }
 
@@ -775,7 +1051,7 @@ __global__ void k_rdm_final(const bass_state* st, double* rho, WsView ws, int fi
 // ---------------------------------------------------------------------------
 template <int KIND, int PASS>
 static cudaError_t launch_tile(OpArgs a, int counter, cudaStream_t s, int* grid_out) {
-  const size_t smem = (size_t)kTilePad * 28 + ((PASS == P_HIST || PASS == P_HIST2) ? kHistBins * 4 : 0);
+  const size_t smem = (size_t)kTilePad * (8 + 16 + 2);
   static int grid = 0;
   if (grid == 0) {
     cudaError_t e = cudaFuncSetAttribute(k_tile<KIND, PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -810,18 +1086,24 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, cudaSt
     KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, 1), 256, 0, s>>>(a, KIND));
   }
   if constexpr (KIND != K_PERM) {
+    constexpr int ns = slots_per_entry(KIND);
+    const int gs = device().sms * 4;
     int gh = 0;
     if ((e = launch_tile<KIND, P_HIST>(a, 0, s, &gh)) != cudaSuccess) return e;
+    KLAUNCH(S_SLOT_HIST1, s, k_slot_hist<1><<<gs, 256, 0, s>>>(a, ns, gh));
     KLAUNCH(S_SELECT1, s, k_select1<<<1, 1024, 0, s>>>(a, gh));
-    if ((e = launch_tile<KIND, P_HIST2>(a, 1, s, nullptr)) != cudaSuccess) return e;
+    KLAUNCH(S_SLOT_HIST2, s, k_slot_hist<2><<<gs, 256, 0, s>>>(a, ns, gh));
     KLAUNCH(S_SELECT2, s, k_select2<<<1, 1024, 0, s>>>(a));
-    if ((e = launch_tile<KIND, P_GATHER>(a, 2, s, nullptr)) != cudaSuccess) return e;
+    KLAUNCH(S_SLOT_GATHER, s, k_slot_gather<<<gs, 256, 0, s>>>(a, ns));
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(k_select_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, kCandSmem * 16);
+      e = cudaFuncSetAttribute(k_select_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, kCandSmem * 16);
+      if (e != cudaSuccess) return e;
       attr = true;
     }
-    KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a));
+    KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a, 0));
+    if ((e = launch_tile<KIND, P_GATHER>(a, 2, s, nullptr)) != cudaSuccess) return e;
+    KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a, 1));
   }
   int gw = 0;
   if ((e = launch_tile<KIND, P_WRITE>(a, 3, s, &gw)) != cudaSuccess) return e;

@@ -115,7 +115,9 @@ typedef struct bass_trunc {
 size_t bass_state_bytes(void);
 size_t bass_ctrl_bytes(void);
 /* workspace for ops whose inputs hold at most max_in entries and whose
-   outputs at most max_out entries (before truncation) */
+   outputs at most max_out entries (before truncation); it is sized for
+   max(4 * max_in, max_out) entries, since the evaluation pass of a 2-qubit
+   gate keeps four 8-byte |a|^2 slots per input entry */
 size_t bass_workspace_bytes(int64_t max_in, int64_t max_out, int num_qubits);
 
 /* ---- state management ----------------------------------------------------- */

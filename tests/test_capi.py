@@ -41,9 +41,10 @@ def test_layouts(native):
 
 def test_workspace_sizes_monotone(native):
     L = native.load_library()
-    sizes = [L.bass_workspace_bytes(n, n, 40) for n in (1, 1000, 1 << 16, 1 << 22)]
+    sizes = [L.bass_workspace_bytes(n, 4 * n, 40) for n in (1, 1000, 1 << 16, 1 << 22)]
     assert sizes == sorted(sizes)
-    assert sizes[-1] < 64 * (1 << 22) + (64 << 20)   # about 45 bytes per entry
+    assert sizes[-1] < 64 * (4 << 22) + (64 << 20)   # about 45 bytes per output entry
+    assert L.bass_workspace_bytes(1000, 1000, 40) == L.bass_workspace_bytes(1000, 4000, 40)
 
 
 def test_lcg_choose_matches_reference_rule(native, orc):
