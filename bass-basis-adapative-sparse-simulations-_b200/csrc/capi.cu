@@ -339,9 +339,10 @@ int bass_rotate_step(bass_state* cur, bass_state* tmp, const double* host_U, int
   bass_trunc tr{};
   tr.k_cond = k;
   tr.k_keep = k;
+  tr.trace = trace;
   cudaError_t e = run_merge_op(K_ROT1, a, tr, 1, j, s);
   if (e == cudaSuccess && trace) e = run_fingerprint(tmp, kSigPmin, nullptr, v, s, ctrl, 1, 0);
-  if (e == cudaSuccess) e = run_decide(cur, tmp, ctrl, v, j, trace, s);
+  if (e == cudaSuccess) e = run_commit(cur, tmp, ctrl, v, j, trace, s);
   return status_of(e);
 }
 

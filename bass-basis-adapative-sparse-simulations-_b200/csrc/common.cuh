@@ -43,7 +43,8 @@ __device__ __forceinline__ void set_error(bass_ctrl* c, int code) {
 // ---------------------------------------------------------------------------
 // exact accumulation
 // ---------------------------------------------------------------------------
-__host__ __device__ __forceinline__ i128 fx_from(double v) {
+// fx_from(v) = trunc(|v| * 2^96) with the sign of v (terms below 2^-96 vanish).
+__host__ __device__ __forceinline__ i128 fx_from_bits(double v) {
   uint64_t b;
 #ifdef __CUDA_ARCH__
   b = (uint64_t)__double_as_longlong(v);
@@ -59,6 +60,24 @@ __host__ __device__ __forceinline__ i128 fx_from(double v) {
   else if (sh > -64) r = (i128)(m >> (-sh));
   else r = 0;
   return (b >> 63) ? -r : r;
+}
+
+// On the device, for |v| < 2^31 (every probability and moment summed here),
+// the same integer is formed in exact floating-point steps: hi =
+// floor(|v| * 2^32) and lo = floor(frac(|v| * 2^32) * 2^64); both scalings are
+// by powers of two and x - floor(x) is exact, so nothing is rounded.
+__host__ __device__ __forceinline__ i128 fx_from(double v) {
+#ifdef __CUDA_ARCH__
+  const double x = __dmul_rn(fabs(v), 4294967296.0);
+  if (!(x < 9223372036854775808.0)) return fx_from_bits(v);
+  const unsigned long long hi = __double2ull_rz(x);
+  const double r = __dsub_rn(x, __ull2double_rn(hi));
+  const unsigned long long lo = __double2ull_rz(__dmul_rn(r, 18446744073709551616.0));
+  const i128 m = (i128)(((u128)hi << 64) | (u128)lo);
+  return v < 0.0 ? -m : m;
+#else
+  return fx_from_bits(v);
+#endif
 }
 
 __device__ __forceinline__ int clz128(u128 u) {
@@ -300,6 +319,33 @@ __device__ __forceinline__ void hist_add(unsigned int* h, unsigned bin, bool val
   if (valid && (__ffs(peers) - 1) == lane) atomicAdd(&h[bin], (unsigned)__popc(peers));
 }
 
+// Calls f(bits, index) for every slot of slots[0, nslots), four 16-byte loads
+// in flight per thread.  Loop bounds are uniform per warp and every lane
+// calls f the same number of times (out-of-range lanes get bits = ~0), so f
+// may use warp-synchronous primitives.
+template <class F>
+__device__ __forceinline__ void scan_slots(const unsigned long long* slots, long long nslots, F&& f) {
+  const ulonglong2* v = reinterpret_cast<const ulonglong2*>(slots);
+  const long long n2 = nslots >> 1;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long b = (long long)blockIdx.x * blockDim.x; b < n2; b += 4 * stride) {
+    ulonglong2 x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const long long i = b + u * stride + threadIdx.x;
+      x[u] = (i < n2) ? v[i] : make_ulonglong2(~0ULL, ~0ULL);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const long long i = b + u * stride + threadIdx.x;
+      f(x[u].x, 2 * i);
+      f(x[u].y, 2 * i + 1);
+    }
+  }
+  if ((nslots & 1) && blockIdx.x == 0 && threadIdx.x < 32)
+    f(threadIdx.x == 0 ? slots[nslots - 1] : ~0ULL, nslots - 1);
+}
+
 // ---------------------------------------------------------------------------
 // workspace
 // ---------------------------------------------------------------------------
@@ -326,13 +372,13 @@ struct SelState {
                          // 4 exact tie at bits == prefix: settle by true key
   int cand_overflow;
   int pad;               // K_IDENT guard: a zero amplitude was produced
-  double total;          // exact sum of |a|^2 over the op's output (before truncation)
-  double total_p2;       // exact sum of |a|^4 over the op's output (before truncation)
+  double total;          // exact sum of |a|^2 over the op's output (truncating ops only)
   long long n_written;
-  double kept;
-  double kept_p2;
+  double kept;           // exact sum of |a|^2 over the kept children
+  double kept_p2;        // ... of |a|^4 (rotation steps)
   int skip_write;        // the write pass has nothing to do (rejected rotation)
-  int pad2;
+  int accept;            // rotation step: the candidate lowers PR
+  double pr_new;         // rotation step: PR of the candidate
 };
 
 struct WsView {

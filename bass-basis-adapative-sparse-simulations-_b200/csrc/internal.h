@@ -31,7 +31,7 @@ struct OpArgs {
 enum Slot {
   S_PARTITION = 30, S_SELECT1 = 31, S_SELECT2 = 32, S_SELECT_EXACT = 33, S_FINALIZE = 34, S_REDUCE = 35,
   S_FINGERPRINT = 36, S_PHASE2Q = 37, S_PHASE1Q = 38, S_RDM_FINAL = 39, S_SORT = 40, S_MERGE_RUNS = 41,
-  S_SMALL = 42, S_SLOT_HIST1 = 43, S_SLOT_HIST2 = 44, S_SLOT_GATHER = 45
+  S_SMALL = 42, S_SLOT_HIST1 = 43, S_SLOT_HIST2 = 44, S_SLOT_GATHER = 45, S_SLOT_KEPT = 46
 };
 
 // Brackets one kernel launch: counts it and, when profiling is on, records
@@ -71,6 +71,9 @@ cudaError_t zero_small(const WsView& ws, cudaStream_t s);
 cudaError_t run_rdm_prepared(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
                              cudaStream_t s);
 cudaError_t run_ident_write(OpArgs a, cudaStream_t s);
+// rotation step: keep the candidate in *tmp if the decision accepted it
+cudaError_t run_commit(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const WsView& ws, int j, int trace,
+                       cudaStream_t s);
 
 // misc.cu
 cudaError_t run_reduce(const bass_state* st, int mode, double* dest, bass_ctrl* ctrl,
@@ -80,8 +83,6 @@ cudaError_t run_fingerprint(const bass_state* st, double pmin, uint64_t* out6, c
 cudaError_t run_radix_sort(uint64_t* keys, double2* amps, long long n, const long long* n_dev,
                            int key_bits, const WsView& ws, bass_ctrl* ctrl, cudaStream_t s);
 cudaError_t run_renorm(bass_state* st, bass_ctrl* ctrl, const WsView& ws, cudaStream_t s);
-cudaError_t run_decide(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const WsView& ws, int j,
-                       int trace, cudaStream_t s);
 cudaError_t run_phase2q(bass_state* st, const double* d, int q1, int q2, bass_ctrl* ctrl, cudaStream_t s);
 cudaError_t run_phase1q(bass_state* st, bass_state* tmp, const double* g, int q, bass_ctrl* ctrl,
                         const WsView& ws, cudaStream_t s);

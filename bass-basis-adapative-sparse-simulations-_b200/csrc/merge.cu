@@ -229,15 +229,17 @@ __host__ __device__ constexpr int slots_per_entry(int kind) {
 // the tile kernel
 // ---------------------------------------------------------------------------
 // Passes: P_HIST (evaluate every child once: its |a|^2 bits go to the slot
-// array, plus exact count / mass sums), P_GATHER (only on an exact tie at the
-// threshold: collect (bits, true key) of the tied children), P_WRITE (write
-// the kept children in order), P_RDM (per-qubit moments).
+// array, plus the child count), P_GATHER (only on an exact tie at the
+// threshold: collect (bits, true key) of the tied children), P_WRITE (count
+// the kept children of every group from the slot array, then evaluate and
+// write the groups that keep any, in order), P_RDM (per-qubit moments).
 template <int KIND, int PASS>
-__global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  uint64_t* sZ = reinterpret_cast<uint64_t*>(smem);
-  double2* sA = reinterpret_cast<double2*>(sZ + kTile);
-  uint16_t* sIdx = reinterpret_cast<uint16_t*>(sA + kTile);
+  double2* sA = reinterpret_cast<double2*>(smem);
+  uint64_t* sZ = reinterpret_cast<uint64_t*>(sA + kTilePad);
+  uint64_t* sK = sZ + kTilePad;
+  uint16_t* sIdx = reinterpret_cast<uint16_t*>(sK + kTilePad);
   __shared__ Hdr H;
   __shared__ SelState S;
   __shared__ long long sItem, sBase, sZstart;
@@ -277,7 +279,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
   }
   const bool scaled = !(H.r0 == 1.0 && H.r1 == 1.0);
   const long long nitems = (KIND == K_RDM) ? ntiles * a.nsets : ntiles;
-  i128 acc[2] = {0, 0};
   long long cnt = 0;
   const int base_e = tid * kPerThread;
 
@@ -334,45 +335,45 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
     __syncthreads();
     const int E = (int)sSegOff[5];
 
-    // ---- load: Z keys and amplitudes (pending renormalisation applied) -----
-    // All of a thread's loads are issued before its shared-memory stores.
-    const int o1 = (int)sSegOff[1], o2 = (int)sSegOff[2], o3 = (int)sSegOff[3], o4 = (int)sSegOff[4];
+    // ---- load: asynchronous copies straight into shared memory -------------
+    {
+      const int o1 = (int)sSegOff[1], o2 = (int)sSegOff[2], o3 = (int)sSegOff[3], o4 = (int)sSegOff[4];
+      const unsigned zb = (unsigned)__cvta_generic_to_shared(sZ);
+      const unsigned ab = (unsigned)__cvta_generic_to_shared(sA);
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      constexpr int L = kPerThread / 2;
-      uint64_t ry[L];
-      double2 rv[L];
-#pragma unroll
-      for (int k = 0; k < L; ++k) {
-        const int e = (half * L + k) * kThreads + tid;
+      for (int k = 0; k < kPerThread; ++k) {
+        const int e = k * kThreads + tid;
         if (e < E) {
           const int sg = (e >= o1) + (e >= o2) + (e >= o3) + (e >= o4);
           const long long src = sSegLo[sg] + (e - sSegOff[sg]);
-          ry[k] = H.keys[src];
-          rv[k] = H.amps[src];
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(zb + 8u * e), "l"(H.keys + src) : "memory");
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(ab + 16u * e), "l"(H.amps + src)
+                       : "memory");
         }
       }
-#pragma unroll
-      for (int k = 0; k < L; ++k) {
-        const int e = (half * L + k) * kThreads + tid;
-        if (e < E) {
-          sZ[e] = (KIND == K_IDENT) ? ry[k] : zmove(ry[k], t, gb);
-          sA[e] = scaled ? scale_load(rv[k], H.r0, H.r1) : rv[k];
-        }
-      }
+      asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
+    if (KIND == K_IDENT && scaled) {
+      for (int e = tid; e < E; e += kThreads) sA[e] = scale_load(sA[e], H.r0, H.r1);
+      __syncthreads();
+    }
 
     // ---- Z order: stable split by the target bit, merge, write back --------
+    // The split moves the Z keys (zmove of the loaded keys) into sK, bit-clear
+    // run first, with their load positions in sIdx; the merge then reads keys
+    // from sK alone and gathers the amplitudes once at the end.
     if (KIND != K_IDENT) {
       const int lane = tid & 31, w = tid >> 5;
       const unsigned lt = (1u << lane) - 1;
       unsigned m0[kPerThread];
+      uint64_t zk[kPerThread];
       int c0 = 0;
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
         const int e = w * 256 + k * 32 + lane;
-        const bool is0 = e < E && !((sZ[e] >> gb) & 1ULL);
+        zk[k] = e < E ? zmove(sZ[e], t, gb) : ~0ULL;
+        const bool is0 = e < E && !((zk[k] >> gb) & 1ULL);
         m0[k] = __ballot_sync(0xffffffffu, is0);
         c0 += __popc(m0[k]);
       }
@@ -392,42 +393,48 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
         const int e = w * 256 + k * 32 + lane;
         const unsigned ones = __ballot_sync(0xffffffffu, e < E) & ~m0[k];
         if (e < E) {
-          if ((m0[k] >> lane) & 1u) sIdx[r0 + __popc(m0[k] & lt)] = (uint16_t)e;
-          else sIdx[n0 + r1 + __popc(ones & lt)] = (uint16_t)e;
+          const int dst = ((m0[k] >> lane) & 1u) ? r0 + __popc(m0[k] & lt) : n0 + r1 + __popc(ones & lt);
+          sK[dst] = zk[k];
+          sIdx[dst] = (uint16_t)e;
         }
         r0 += __popc(m0[k]);
         r1 += __popc(ones);
       }
       __syncthreads();
       const int n1 = E - n0;
-      const uint16_t* S0 = sIdx;
-      const uint16_t* S1 = sIdx + n0;
+      const uint64_t* K0 = sK;
+      const uint64_t* K1 = sK + n0;
       const int d = base_e < E ? base_e : E;
       int lo = d - n1 > 0 ? d - n1 : 0, hi = d < n0 ? d : n0;
       while (lo < hi) {
         const int m = (lo + hi) >> 1;
-        if (sZ[S0[m]] < sZ[S1[d - 1 - m]]) lo = m + 1;
+        if (K0[m] < K1[d - 1 - m]) lo = m + 1;
         else hi = m;
       }
       int i = lo, j = d - lo;
       uint64_t rz[kPerThread];
+      int rs[kPerThread];
+      uint64_t z0 = (i < n0) ? K0[i] : ~0ULL;
+      uint64_t z1 = (j < n1) ? K1[j] : ~0ULL;
+#pragma unroll
+      for (int k = 0; k < kPerThread; ++k) {
+        const bool take0 = z0 < z1;
+        rz[k] = take0 ? z0 : z1;
+        rs[k] = take0 ? i : n0 + j;
+        if (take0) {
+          ++i;
+          z0 = (i < n0) ? K0[i] : ~0ULL;
+        } else {
+          ++j;
+          z1 = (j < n1) ? K1[j] : ~0ULL;
+        }
+      }
       double2 ra[kPerThread];
-      uint64_t z0 = (i < n0) ? sZ[S0[i]] : ~0ULL;
-      uint64_t z1 = (j < n1) ? sZ[S1[j]] : ~0ULL;
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
         if (d + k < E) {
-          if (z0 < z1) {
-            rz[k] = z0;
-            ra[k] = sA[S0[i]];
-            ++i;
-            z0 = (i < n0) ? sZ[S0[i]] : ~0ULL;
-          } else {
-            rz[k] = z1;
-            ra[k] = sA[S1[j]];
-            ++j;
-            z1 = (j < n1) ? sZ[S1[j]] : ~0ULL;
-          }
+          const double2 v = sA[sIdx[rs[k]]];
+          ra[k] = scaled ? scale_load(v, H.r0, H.r1) : v;
         }
       }
       __syncthreads();
@@ -475,14 +482,27 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
       double2 ca[MC];
       uint16_t* sOff = sIdx;  // free after the merge
       // (a) kept children per position
+      constexpr bool kFromSlots = KIND == K_GATE1 || KIND == K_ROT1 || KIND == K_GATE2;
+      const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys) + NS * sZstart;
       for (int p = tid; p < E; p += kThreads) {
-        const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
         int kc = 0;
+        if (kFromSlots) {
+          // a group start holds its children's |a|^2 bits, other positions ~0
+          unsigned long long sb[NS];
 #pragma unroll
-        for (int c = 0; c < MC; ++c)
-          if (((cm >> c) & 1u) &&
-              keep_child((uint64_t)__double_as_longlong(prob(ca[c])), kb | (uint64_t)c, S, H.qat_out))
-            ++kc;
+          for (int c = 0; c < NS; c += 2) {
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(slots + (long long)NS * p + c);
+            sb[c] = v.x;
+            sb[c + 1] = v.y;
+          }
+          const uint64_t base = (sZ[p] >> (gb + 1)) << (gb + 1);
+#pragma unroll
+          for (int c = 0; c < NS; ++c)
+            if (sb[c] != ~0ULL && keep_child(sb[c], base | (uint64_t)c, S, H.qat_out)) ++kc;
+        } else {
+          const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+          if ((cm & 1u) && keep_child((uint64_t)__double_as_longlong(prob(ca[0])), kb, S, H.qat_out)) kc = 1;
+        }
         sOff[p] = (uint16_t)kc;
       }
       __syncthreads();
@@ -531,8 +551,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
               ok[o] = kb | (uint64_t)c;
               oa[o] = ca[c];
               ++o;
-              acc[0] += fx_from(pv);
-              ++cnt;
             }
           }
         }
@@ -547,10 +565,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
 #pragma unroll
         for (int c = 0; c < NS; ++c) {
           if ((cm >> c) & 1u) {
-            const double pv = prob(ca[c]);
-            sb[c] = (unsigned long long)__double_as_longlong(pv);
-            acc[0] += fx_from(pv);
-            acc[1] += fx_from(__dmul_rn(pv, pv));
+            sb[c] = (unsigned long long)__double_as_longlong(prob(ca[c]));
             ++cnt;
           } else {
             sb[c] = ~0ULL;
@@ -590,15 +605,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
     __syncthreads();
   }
 
-  // ---- flush ---------------------------------------------------------------
-  if (PASS == P_HIST || PASS == P_WRITE) {
-    i128 v[3] = {acc[0], acc[1], (i128)cnt};
-    block_sum_i128<3>(v, sRed);
+  // ---- flush: the CTA's child count ----------------------------------------
+  if (PASS == P_HIST) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    if ((tid & 31) == 0) reinterpret_cast<long long*>(sRed)[tid >> 5] = cnt;
+    __syncthreads();
     if (tid == 0) {
-      Partial* pt = a.ws.partials + blockIdx.x;
-      pt->s[0] = v[0];
-      pt->s[1] = v[1];
-      pt->c[0] = (long long)v[2];
+      long long c = 0;
+      for (int w = 0; w < kThreads / 32; ++w) c += reinterpret_cast<long long*>(sRed)[w];
+      a.ws.partials[blockIdx.x].c[0] = c;
     }
   }
 }
@@ -607,9 +623,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(OpArgs a) {
 // streaming passes over the slot array (one |a|^2 bit pattern per child,
 // ~0 where a group has fewer children than slots)
 // ---------------------------------------------------------------------------
-// LEVEL 1: histogram of bits >> 50 over all slots, only when the op
-// truncates (count from the evaluation pass's per-CTA partials); LEVEL 2:
-// bits 37-49 of the slots inside the level-1 boundary bin.
+// LEVEL 1: histogram of bits >> 50 over all slots and the exact mass of all
+// children, only when the op truncates (count from the evaluation pass's
+// per-CTA partials); LEVEL 2: bits 37-49 of the slots inside the level-1
+// boundary bin.
 template <int LEVEL>
 __global__ void __launch_bounds__(256) k_slot_hist(OpArgs a, int ns, int nblk) {
   __shared__ unsigned int h[kHistBins];
@@ -626,7 +643,7 @@ __global__ void __launch_bounds__(256) k_slot_hist(OpArgs a, int ns, int nblk) {
     if (threadIdx.x == 0) {
       long long n_out = 0;
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) n_out += sCnt[w];
-      sGo = !(a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out || a.k_keep <= 0);
+      sGo = !(a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out);
       sPrefix = 0;
     }
   } else if (threadIdx.x == 0) {
@@ -641,12 +658,17 @@ __global__ void __launch_bounds__(256) k_slot_hist(OpArgs a, int ns, int nblk) {
   if (nslots > a.ws.max_n) return;
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
   const unsigned long long pre = sPrefix;
-  for (long long b = (long long)blockIdx.x * blockDim.x; b < nslots; b += (long long)gridDim.x * blockDim.x) {
-    const long long i = b + threadIdx.x;
-    const unsigned long long bits = (i < nslots) ? slots[i] : ~0ULL;
+  i128 v[1] = {0};
+  scan_slots(slots, nslots, [&](unsigned long long bits, long long) {
     const bool valid = bits != ~0ULL && (LEVEL == 1 || (bits >> 50) == pre);
     const unsigned bin = LEVEL == 1 ? (unsigned)(bits >> 50) : (unsigned)((bits >> 37) & (kHistBins - 1));
     hist_add(h, bin, valid);
+    if (LEVEL == 1 && valid) v[0] += fx_from(__longlong_as_double((long long)bits));
+  });
+  if (LEVEL == 1) {  // exact mass of all children (the truncation's denominator)
+    __shared__ i128 sRed[8];
+    block_sum_i128<1>(v, sRed);
+    if (threadIdx.x == 0) a.ws.partials[blockIdx.x].s[2] = v[0];
   }
   __syncthreads();
   unsigned int* gh = LEVEL == 1 ? a.ws.hist1 : a.ws.hist2;
@@ -662,9 +684,7 @@ __global__ void __launch_bounds__(256) k_slot_gather(OpArgs a, int ns) {
   const long long nslots = (long long)ns * a.in->nnz;
   if (nslots > a.ws.max_n) return;
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots;
-       i += (long long)gridDim.x * blockDim.x) {
-    const unsigned long long bits = slots[i];
+  scan_slots(slots, nslots, [&](unsigned long long bits, long long i) {
     if (bits != ~0ULL && (bits >> 37) == pre) {
       const unsigned long long k = atomicAdd(reinterpret_cast<unsigned long long*>(&sel->n_cand), 1ULL);
       if ((long long)k < a.ws.max_n) {
@@ -674,6 +694,105 @@ __global__ void __launch_bounds__(256) k_slot_gather(OpArgs a, int ns) {
         sel->cand_overflow = 1;
       }
     }
+  });
+}
+
+// Exact mass (and, for a rotation step, sum of |a|^4) of the children that
+// survive the selection: bits > T, or >= T when every child at T is kept; all
+// children when the op does not truncate.  Per-CTA partials s[0], s[1].
+template <bool P2>
+__global__ void __launch_bounds__(256) k_slot_sums(OpArgs a, int ns) {
+  __shared__ i128 sRed[2 * 8];
+  __shared__ int sTrunc, sInclEq;
+  __shared__ unsigned long long sT;
+  if (threadIdx.x == 0) {
+    const SelState* sel = a.ws.sel;
+    sTrunc = sel->do_trunc;
+    sT = sel->t_bits;
+    sInclEq = sel->t_key == ~0ULL;
+  }
+  __syncthreads();
+  if (!P2 && !sTrunc) return;
+  const long long nslots = (long long)ns * a.in->nnz;
+  if (nslots > a.ws.max_n) return;
+  const unsigned long long T = sTrunc ? sT : 0ULL;
+  const bool incl = !sTrunc || sInclEq;
+  i128 v[2] = {0, 0};
+  scan_slots(reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys), nslots,
+             [&](unsigned long long bits, long long) {
+               if (bits != ~0ULL && (bits > T || (incl && bits == T))) {
+                 const double p = __longlong_as_double((long long)bits);
+                 v[0] += fx_from(p);
+                 if (P2) v[1] += fx_from(__dmul_rn(p, p));
+               }
+             });
+  block_sum_i128<2>(v, sRed);
+  if (threadIdx.x == 0) {
+    Partial* pt = a.ws.partials + blockIdx.x;
+    pt->s[0] = v[0];
+    pt->s[1] = v[1];
+  }
+}
+
+// The kept mass (and sum of |a|^4) from k_slot_sums' partials; ties at T
+// settled by key contribute `need` copies of T.  mode 1 (rotation step, the
+// decision of bass_simulator.py:795-814): the candidate's PR = kept^2 /
+// sum |a|^4 against ctrl->pr_cur; a rejected candidate is not written unless
+// a trace is kept.
+__global__ void k_kept_final(OpArgs a, int nblk, int mode, int j, int trace) {
+  __shared__ i128 sRed[2 * 8];
+  SelState* sel = a.ws.sel;
+  const int trunc = sel->do_trunc;
+  if (mode == 0 && !trunc) return;
+  i128 v[2] = {0, 0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    v[0] += a.ws.partials[b].s[0];
+    v[1] += a.ws.partials[b].s[1];
+  }
+  block_sum_i128<2>(v, sRed);
+  if (threadIdx.x != 0) return;
+  if (trunc && sel->t_key != ~0ULL) {
+    const double T = __longlong_as_double((long long)sel->t_bits);
+    v[0] += (i128)sel->need * fx_from(T);
+    v[1] += (i128)sel->need * fx_from(__dmul_rn(T, T));
+  }
+  const double kept = fx_to(v[0]);
+  const double p2 = fx_to(v[1]);
+  sel->kept = kept;
+  sel->kept_p2 = p2;
+  if (mode != 1) return;
+  const long long n_kept = trunc ? (sel->k_keep > 0 ? sel->k_keep : 0) : sel->n_out;
+  bass_ctrl* c = a.ctrl;
+  const double pr_new = (n_kept == 0 || !(p2 > 0.0)) ? INFINITY : __ddiv_rn(__dmul_rn(kept, kept), p2);
+  const bool reject = pr_new >= c->pr_cur * (1.0 - c->pr_tie_tol);
+  c->frac[j] = kept;
+  c->accept[j] = reject ? 0 : 1;
+  sel->accept = reject ? 0 : 1;
+  sel->pr_new = pr_new;
+  sel->skip_write = (reject && !trace) ? 1 : 0;
+}
+
+// Rotation step, after the write pass: keep the candidate if accepted.
+__global__ void k_commit(bass_state* cur, bass_state* tmp, WsView ws, bass_ctrl* c, int j, int trace) {
+  const SelState* sel = ws.sel;
+  if (!sel->accept) return;
+  bass_state t = *cur;
+  *cur = *tmp;
+  *tmp = t;
+  c->pr_cur = sel->pr_new;
+  const double frac = c->frac[j];
+  c->gamma_running *= sqrt(frac > 1e-30 ? frac : 0.0);
+  if (trace && c->trace) {
+    const long long i = c->trace_len;
+    if (i >= c->trace_cap) {
+      set_error(c, BASS_ERR_CAPACITY);
+      return;
+    }
+    uint64_t* e = c->trace + i * BASS_TRACE_WORDS;
+    e[0] = 1;
+    e[1] = (uint64_t)j;
+    for (int k = 2; k < BASS_TRACE_WORDS; ++k) e[k] = 0;
+    c->trace_len = i + 1;
   }
 }
 
@@ -724,23 +843,21 @@ __device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, 
   return sRes;
 }
 
-__global__ void __launch_bounds__(1024) k_select1(OpArgs a, int nblk) {
+// nblk: CTAs of the evaluation pass (child counts); nblk1: CTAs of the
+// level-1 slot histogram (exact mass of all children, when truncating).
+__global__ void __launch_bounds__(1024) k_select1(OpArgs a, int nblk, int nblk1) {
   __shared__ long long sS[1024];
-  __shared__ i128 sRed[3 * 32];
+  __shared__ i128 sRed[2 * 32];
   SelState* sel = a.ws.sel;
-  i128 v[3] = {0, 0, 0};
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-    v[0] += a.ws.partials[b].s[0];
-    v[1] += a.ws.partials[b].s[1];
-    v[2] += (i128)a.ws.partials[b].c[0];
-  }
-  block_sum_i128<3>(v, sRed);
+  i128 v[2] = {0, 0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) v[1] += (i128)a.ws.partials[b].c[0];
+  for (int b = threadIdx.x; b < nblk1; b += blockDim.x) v[0] += a.ws.partials[b].s[2];
+  block_sum_i128<2>(v, sRed);
   __shared__ int sGo;
   if (threadIdx.x == 0) {
-    const long long n_out = (long long)v[2];
+    const long long n_out = (long long)v[1];
     sel->n_out = n_out;
-    sel->total = fx_to(v[0]);
-    sel->total_p2 = fx_to(v[1]);
+    sel->total = fx_to(v[0]);  // meaningful only when the op truncates
     sel->k_keep = a.k_keep;
     sGo = 0;
     if (a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out) {
@@ -967,17 +1084,15 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
 // ---------------------------------------------------------------------------
 // mode 0: plain op; mode 1: basis-rotation step (always renormalises, keeps
 // the retained mass in sel->kept for the decision)
-__global__ void k_finalize(OpArgs a, bass_trunc tr, int mode, int kind, int nblk) {
-  __shared__ i128 sRed[8];
+// The kept mass comes from k_kept_final (set when the op truncates or is a
+// rotation step, the only cases that use it).
+__global__ void k_finalize(OpArgs a, bass_trunc tr, int mode, int kind) {
   SelState* sel = a.ws.sel;
-  i128 v[1] = {0};
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) v[0] += a.ws.partials[b].s[0];
-  block_sum_i128<1>(v, sRed);
   if (threadIdx.x != 0) return;
   const bass_state* in = a.in;
   bass_state* out = a.out;
   bass_ctrl* c = a.ctrl;
-  const double kept = fx_to(v[0]);
+  const double kept = sel->kept;
   const long long n_in = in->nnz;
   long long nw = sel->n_written;
   if (nw > out->cap) {  // the write pass skipped the tiles that did not fit
@@ -995,7 +1110,6 @@ __global__ void k_finalize(OpArgs a, bass_trunc tr, int mode, int kind, int nblk
   out->nnz = nw;
   out->rscale[0] = 1.0;
   out->rscale[1] = 1.0;
-  sel->kept = kept;
   if (kind == K_PERM) return;  // first pass of a 2-qubit gate: no bookkeeping
   c->amp_updates += n_in;
   c->n_ops += 1;
@@ -1051,7 +1165,7 @@ __global__ void k_rdm_final(const bass_state* st, double* rho, WsView ws, int fi
 // ---------------------------------------------------------------------------
 template <int KIND, int PASS>
 static cudaError_t launch_tile(OpArgs a, int counter, cudaStream_t s, int* grid_out) {
-  const size_t smem = (size_t)kTilePad * (8 + 16 + 2);
+  const size_t smem = (size_t)kTilePad * (16 + 8 + 8 + 2);
   static int grid = 0;
   if (grid == 0) {
     cudaError_t e = cudaFuncSetAttribute(k_tile<KIND, PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1076,7 +1190,7 @@ cudaError_t zero_small(const WsView& ws, cudaStream_t s) {
 }
 
 template <int KIND>
-static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, cudaStream_t s) {
+static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j, cudaStream_t s) {
   cudaError_t e = zero_small(a.ws, s);
   if (e != cudaSuccess) return e;
   a.k_cond = tr.k_cond;
@@ -1091,7 +1205,7 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, cudaSt
     int gh = 0;
     if ((e = launch_tile<KIND, P_HIST>(a, 0, s, &gh)) != cudaSuccess) return e;
     KLAUNCH(S_SLOT_HIST1, s, k_slot_hist<1><<<gs, 256, 0, s>>>(a, ns, gh));
-    KLAUNCH(S_SELECT1, s, k_select1<<<1, 1024, 0, s>>>(a, gh));
+    KLAUNCH(S_SELECT1, s, k_select1<<<1, 1024, 0, s>>>(a, gh, gs));
     KLAUNCH(S_SLOT_HIST2, s, k_slot_hist<2><<<gs, 256, 0, s>>>(a, ns, gh));
     KLAUNCH(S_SELECT2, s, k_select2<<<1, 1024, 0, s>>>(a));
     KLAUNCH(S_SLOT_GATHER, s, k_slot_gather<<<gs, 256, 0, s>>>(a, ns));
@@ -1104,24 +1218,32 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, cudaSt
     KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a, 0));
     if ((e = launch_tile<KIND, P_GATHER>(a, 2, s, nullptr)) != cudaSuccess) return e;
     KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a, 1));
+    if (fin_mode == 1) KLAUNCH(S_SLOT_KEPT, s, k_slot_sums<true><<<gs, 256, 0, s>>>(a, ns));
+    else KLAUNCH(S_SLOT_KEPT, s, k_slot_sums<false><<<gs, 256, 0, s>>>(a, ns));
+    KLAUNCH(S_REDUCE, s, k_kept_final<<<1, 256, 0, s>>>(a, gs, fin_mode, j, tr.trace));
   }
   int gw = 0;
   if ((e = launch_tile<KIND, P_WRITE>(a, 3, s, &gw)) != cudaSuccess) return e;
-  KLAUNCH(S_FINALIZE, s, k_finalize<<<1, 256, 0, s>>>(a, tr, fin_mode, KIND, gw));
+  KLAUNCH(S_FINALIZE, s, k_finalize<<<1, 32, 0, s>>>(a, tr, fin_mode, KIND));
   return cudaGetLastError();
 }
 
 cudaError_t run_merge_op(int kind, OpArgs a, const bass_trunc& tr, int finalize_mode, int j,
                          cudaStream_t s) {
-  (void)j;
   switch (kind) {
-    case K_GATE1: return merge_op<K_GATE1>(a, tr, finalize_mode, s);
-    case K_ROT1: return merge_op<K_ROT1>(a, tr, finalize_mode, s);
-    case K_GATE2: return merge_op<K_GATE2>(a, tr, finalize_mode, s);
-    case K_PERM: return merge_op<K_PERM>(a, tr, finalize_mode, s);
-    case K_IDENT: return merge_op<K_IDENT>(a, tr, finalize_mode, s);
+    case K_GATE1: return merge_op<K_GATE1>(a, tr, finalize_mode, j, s);
+    case K_ROT1: return merge_op<K_ROT1>(a, tr, finalize_mode, j, s);
+    case K_GATE2: return merge_op<K_GATE2>(a, tr, finalize_mode, j, s);
+    case K_PERM: return merge_op<K_PERM>(a, tr, finalize_mode, j, s);
+    case K_IDENT: return merge_op<K_IDENT>(a, tr, finalize_mode, j, s);
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t run_commit(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const WsView& ws, int j, int trace,
+                       cudaStream_t s) {
+  KLAUNCH(S_REDUCE, s, k_commit<<<1, 1, 0, s>>>(cur, tmp, ws, ctrl, j, trace));
+  return cudaGetLastError();
 }
 
 // write pass only (keep everything the drop rule keeps); used by the guarded

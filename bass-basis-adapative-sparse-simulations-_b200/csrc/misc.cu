@@ -139,36 +139,6 @@ __global__ void k_fp_out(WsView ws, uint64_t* out6, bass_ctrl* c, int append, in
 }
 
 // ---------------------------------------------------------------------------
-// basis-rotation decision (bass_simulator.py:795-814)
-// ---------------------------------------------------------------------------
-__global__ void k_decide(bass_state* cur, bass_state* tmp, WsView ws, int nblk, bass_ctrl* c, int j,
-                         int trace) {
-  __shared__ i128 sRed[8];
-  const double S = reduce_red(ws, nblk, sRed);
-  if (threadIdx.x != 0) return;
-  const double pr_new = (tmp->nnz == 0) ? INFINITY : (S > 1e-60 ? 1.0 / S : INFINITY);
-  const double pr = c->pr_cur;
-  const double frac = ws.sel->kept;
-  const bool reject = pr_new >= pr * (1.0 - c->pr_tie_tol);
-  c->frac[j] = frac;
-  c->accept[j] = reject ? 0 : 1;
-  if (reject) return;
-  bass_state t = *cur;
-  *cur = *tmp;
-  *tmp = t;
-  c->pr_cur = pr_new;
-  c->gamma_running *= sqrt(frac > 1e-30 ? frac : 0.0);
-  if (trace && c->trace) {
-    const long long i = c->trace_len;
-    if (i >= c->trace_cap) { set_error(c, BASS_ERR_CAPACITY); return; }
-    uint64_t* e = c->trace + i * BASS_TRACE_WORDS;
-    e[0] = 1; e[1] = (uint64_t)j;
-    for (int k = 2; k < BASS_TRACE_WORDS; ++k) e[k] = 0;
-    c->trace_len = i + 1;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // diagonal gates
 // ---------------------------------------------------------------------------
 // sparse_state.py:178-190: a *= diag[(b_q1 << 1) | b_q2], in place
@@ -593,14 +563,6 @@ cudaError_t run_renorm(bass_state* st, bass_ctrl* ctrl, const WsView& ws, cudaSt
   KLAUNCH(S_REDUCE, s, k_reduce_state<R_NORM2><<<grid, 256, 0, s>>>(st, ws));
   KLAUNCH(S_REDUCE, s, k_renorm_apply<<<1, 256, 0, s>>>(st, ws, grid));
   KLAUNCH(S_SMALL, s, k_materialize<<<device().sms * 4, 256, 0, s>>>(st, ws, ctrl));
-  return cudaGetLastError();
-}
-
-cudaError_t run_decide(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const WsView& ws, int j,
-                       int trace, cudaStream_t s) {
-  const int grid = device().grid_small > 1024 ? 1024 : device().grid_small;
-  KLAUNCH(S_REDUCE, s, k_reduce_state<R_P2><<<grid, 256, 0, s>>>(tmp, ws));
-  KLAUNCH(S_REDUCE, s, k_decide<<<1, 256, 0, s>>>(cur, tmp, ws, grid, ctrl, j, trace));
   return cudaGetLastError();
 }
 

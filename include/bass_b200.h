@@ -206,7 +206,10 @@ int bass_rdm_1q_noalloc(const bass_state* st, int64_t max_entries, int num_qubit
    *cur by host_U (2x2) into *tmp (bass_simulator.py:156-199), keep the top k
    (:565-572), renormalise (:551-554), compare PR with ctrl->pr_cur and keep the
    rotated state (swapping the contents of *cur and *tmp) only if it lowers PR
-   by more than ctrl->pr_tie_tol.  Records ctrl->accept[j], ctrl->frac[j]. */
+   by more than ctrl->pr_tie_tol.  Records ctrl->accept[j], ctrl->frac[j].
+   The candidate's PR is frac^2 / sum |a|^4 over the kept children (exact
+   sums), decided before the candidate is written: a rejected candidate is
+   written to *tmp only when trace != 0 (its fingerprint goes to the trace). */
 int bass_rotate_step(bass_state* cur, bass_state* tmp, const double* host_U, int j, int64_t k,
                      int trace, bass_ctrl* ctrl, void* ws, size_t ws_bytes, void* stream);
 /* Order-independent key-set fingerprints of a state: out[0..2] over all keys,

@@ -459,8 +459,12 @@ class OracleBASS:
                 st.x, st.alpha = rotate_1q(st.x, st.alpha, j, V.conj().T)
                 self._truncate_state(st)
                 frac = sum_p(st.alpha)
+                p2 = sum_p2(st.alpha)
                 self._renorm(st)
-                pr_new = self._pr(st)
+                # PR of the renormalised candidate, from the exact sums of the
+                # unnormalised one: frac^2 / sum |a|^4 (the reference evaluates
+                # 1 / sum |a/sqrt(frac)|^4; the two differ by rounding only)
+                pr_new = (frac * frac) / p2 if (st.nnz > 0 and p2 > 0) else float("inf")
                 # the reference's rule is `pr_new >= pr`; a rotation must lower
                 # PR by more than pr_tie_tol (relative) to count (0 restores it)
                 if pr_new >= pr * (1.0 - self.pr_tie_tol):

@@ -240,8 +240,8 @@ def test_rotation_step_matches_oracle(B, orc):
         xr, ar = orc.rotate_1q(x, a, j, V.conj().T)
         xt, at, _, _ = orc.select_topk(xr, ar, k)
         frac = orc.sum_p(at)
+        pr_new = frac * frac / orc.sum_p2(at)
         at = at / np.sqrt(frac)
-        pr_new = 1.0 / orc.sum_p2(at)
         pr = 1.0 / orc.sum_p2(a)
         acc = not (pr_new >= pr * (1.0 - 1e-12))
         assert int(c["accept"][j]) == int(acc)
