@@ -379,6 +379,8 @@ struct SelState {
   int skip_write;        // the write pass has nothing to do (rejected rotation)
   int accept;            // rotation step: the candidate lowers PR
   double pr_new;         // rotation step: PR of the candidate
+  int tie;               // the threshold was settled by key (stage 4 was taken)
+  int pad3;
 };
 
 struct WsView {

@@ -25,6 +25,7 @@ struct OpArgs {
   int drop_zero;  // K_IDENT: drop entries whose amplitude is exactly zero
   int guard;      // K_IDENT: run only if ws.sel->pad (zero flag) is set
   int prof;       // count entries into ctrl->prof_in / prof_out
+  int write_mode; // P_WRITE: 0 look-back + drop rule, 1 slot array + tile offsets, 2 one child per entry
   long long k_cond, k_keep;
 };
 

@@ -221,6 +221,17 @@ __device__ __forceinline__ bool keep_child(uint64_t bits, uint64_t key, const Se
   return S.t_key == ~0ULL || true_key(key, qat, 64) <= S.t_key;
 }
 
+// Slot value of a child at the threshold that survives the key tie-break:
+// above every probability's bit pattern (a NaN payload) and distinct from ~0.
+constexpr unsigned long long kSlotKeptTie = 0x7FFFFFFFFFFFFFFEULL;
+
+// Does the child with this slot survive the selection?  (T, incl) = (t_bits,
+// t_key == ~0) when truncating, (0, true) otherwise; ties settled by key were
+// rewritten to kSlotKeptTie / 0 by k_tie_mark.
+__device__ __forceinline__ bool slot_kept(unsigned long long bits, unsigned long long T, bool incl) {
+  return bits != ~0ULL && (bits > T || (incl && bits == T));
+}
+
 __host__ __device__ constexpr int slots_per_entry(int kind) {
   return kind == K_GATE2 ? 4 : (kind == K_GATE1 || kind == K_ROT1) ? 2 : 1;
 }
@@ -230,9 +241,9 @@ __host__ __device__ constexpr int slots_per_entry(int kind) {
 // ---------------------------------------------------------------------------
 // Passes: P_HIST (evaluate every child once: its |a|^2 bits go to the slot
 // array, plus the child count), P_GATHER (only on an exact tie at the
-// threshold: collect (bits, true key) of the tied children), P_WRITE (count
-// the kept children of every group from the slot array, then evaluate and
-// write the groups that keep any, in order), P_RDM (per-qubit moments).
+// threshold: collect (slot index, true key) of the tied children), P_WRITE
+// (the kept-children mask of every group from the slot array, then evaluate
+// and write the groups that keep any, in order), P_RDM (per-qubit moments).
 template <int KIND, int PASS>
 __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -477,33 +488,44 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
         pt->s[0] = v[0]; pt->s[1] = v[1]; pt->s[2] = v[2]; pt->s[3] = v[3];
       }
     } else if (PASS == P_WRITE) {
+      // write_mode 1: kept children from the slot array, tile base from
+      //   k_scan_tiles; 2: one child per entry, base = the tile's Z start;
+      //   0: the drop rule decides, base by decoupled look-back.
       constexpr int MC = KindTraits<KIND>::kMaxChildren;
       uint64_t kb;
       double2 ca[MC];
-      uint16_t* sOff = sIdx;  // free after the merge
-      // (a) kept children per position
-      constexpr bool kFromSlots = KIND == K_GATE1 || KIND == K_ROT1 || KIND == K_GATE2;
+      uint16_t* sOff = sIdx;                              // free after the merge
+      uint8_t* sMask = reinterpret_cast<uint8_t*>(sK);    // free after the merge
+      const int wmode = a.write_mode;
+      const unsigned long long T = S.do_trunc ? S.t_bits : 0ULL;
+      const bool incl = !S.do_trunc || S.t_key == ~0ULL;
       const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys) + NS * sZstart;
+      // (a) kept-children mask per position
       for (int p = tid; p < E; p += kThreads) {
-        int kc = 0;
-        if (kFromSlots) {
-          // a group start holds its children's |a|^2 bits, other positions ~0
+        unsigned mk = 0;
+        if (wmode == 1) {
           unsigned long long sb[NS];
+          if (NS == 1) {
+            sb[0] = slots[p];
+          } else {
 #pragma unroll
-          for (int c = 0; c < NS; c += 2) {
-            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(slots + (long long)NS * p + c);
-            sb[c] = v.x;
-            sb[c + 1] = v.y;
+            for (int c = 0; c < NS; c += 2) {
+              const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(slots + (long long)NS * p + c);
+              sb[c] = v.x;
+              sb[c + 1] = v.y;
+            }
           }
-          const uint64_t base = (sZ[p] >> (gb + 1)) << (gb + 1);
 #pragma unroll
           for (int c = 0; c < NS; ++c)
-            if (sb[c] != ~0ULL && keep_child(sb[c], base | (uint64_t)c, S, H.qat_out)) ++kc;
+            if (slot_kept(sb[c], T, incl)) mk |= 1u << c;
+        } else if (wmode == 2) {
+          mk = 1u;
         } else {
           const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
-          if ((cm & 1u) && keep_child((uint64_t)__double_as_longlong(prob(ca[0])), kb, S, H.qat_out)) kc = 1;
+          if ((cm & 1u) && keep_child((uint64_t)__double_as_longlong(prob(ca[0])), kb, S, H.qat_out)) mk = 1u;
         }
-        sOff[p] = (uint16_t)kc;
+        sMask[p] = (uint8_t)mk;
+        sOff[p] = (uint16_t)__popc(mk);
       }
       __syncthreads();
       // (b) counts -> exclusive offsets in place (position order)
@@ -523,31 +545,34 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
         }
       }
       // (c) the tile's base in the output
-      if (tid < 32) {
-        const long long b = lookback_warp(a.ws.status, tile, tile_total, a.ctrl);
-        if (tid == 0) {
-          sBase = b;
-          if (tile == ntiles - 1) a.ws.sel->n_written = b + tile_total;
-          if (b + tile_total > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
-          if (a.prof) atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_out[KIND * 5 + PASS]),
-                                (unsigned long long)tile_total);
+      if (wmode == 0) {
+        if (tid < 32) {
+          const long long b = lookback_warp(a.ws.status, tile, tile_total, a.ctrl);
+          if (tid == 0) sBase = b;
         }
+      } else if (tid == 0) {
+        sBase = (wmode == 1) ? (long long)a.ws.status[tile] : sZstart;
       }
       __syncthreads();
+      if (tid == 0) {
+        const long long b = sBase;
+        if (tile == ntiles - 1) a.ws.sel->n_written = b + tile_total;
+        if (b + tile_total > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
+        if (a.prof) atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_out[KIND * 5 + PASS]),
+                              (unsigned long long)tile_total);
+      }
       // (d) write the kept children
       if (sBase + tile_total <= a.out->cap) {
         uint64_t* ok = a.out->keys;
         double2* oa = reinterpret_cast<double2*>(a.out->amps);
         for (int p = tid; p < E; p += kThreads) {
-          const int o_end = (p + 1 < E) ? sOff[p + 1] : tile_total;
-          if (o_end == sOff[p]) continue;
+          const unsigned mk = sMask[p];
+          if (!mk) continue;
           long long o = sBase + sOff[p];
-          const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+          group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
 #pragma unroll
           for (int c = 0; c < MC; ++c) {
-            if (!((cm >> c) & 1u)) continue;
-            const double pv = prob(ca[c]);
-            if (keep_child((uint64_t)__double_as_longlong(pv), kb | (uint64_t)c, S, H.qat_out)) {
+            if ((mk >> c) & 1u) {
               ok[o] = kb | (uint64_t)c;
               oa[o] = ca[c];
               ++o;
@@ -593,7 +618,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
             const unsigned long long slot =
                 atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws.sel->n_cand), 1ULL);
             if ((long long)slot < a.ws.max_n) {
-              a.ws.cand_bits[slot] = bits;
+              a.ws.cand_bits[slot] = (unsigned long long)(NS * (sZstart + p) + c);  // its slot index
               a.ws.cand_key[slot] = true_key(kb | (uint64_t)c, H.qat_out, 64);
             } else {
               a.ws.sel->cand_overflow = 1;
@@ -623,10 +648,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
 // streaming passes over the slot array (one |a|^2 bit pattern per child,
 // ~0 where a group has fewer children than slots)
 // ---------------------------------------------------------------------------
-// LEVEL 1: histogram of bits >> 50 over all slots and the exact mass of all
-// children, only when the op truncates (count from the evaluation pass's
-// per-CTA partials); LEVEL 2: bits 37-49 of the slots inside the level-1
-// boundary bin.
+// LEVEL 1: histogram of bits >> 50 over all slots, only when the op
+// truncates (count from the evaluation pass's per-CTA partials); LEVEL 2:
+// bits 37-49 of the slots inside the level-1 boundary bin.
 template <int LEVEL>
 __global__ void __launch_bounds__(256) k_slot_hist(OpArgs a, int ns, int nblk) {
   __shared__ unsigned int h[kHistBins];
@@ -658,18 +682,11 @@ __global__ void __launch_bounds__(256) k_slot_hist(OpArgs a, int ns, int nblk) {
   if (nslots > a.ws.max_n) return;
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
   const unsigned long long pre = sPrefix;
-  i128 v[1] = {0};
   scan_slots(slots, nslots, [&](unsigned long long bits, long long) {
     const bool valid = bits != ~0ULL && (LEVEL == 1 || (bits >> 50) == pre);
     const unsigned bin = LEVEL == 1 ? (unsigned)(bits >> 50) : (unsigned)((bits >> 37) & (kHistBins - 1));
     hist_add(h, bin, valid);
-    if (LEVEL == 1 && valid) v[0] += fx_from(__longlong_as_double((long long)bits));
   });
-  if (LEVEL == 1) {  // exact mass of all children (the truncation's denominator)
-    __shared__ i128 sRed[8];
-    block_sum_i128<1>(v, sRed);
-    if (threadIdx.x == 0) a.ws.partials[blockIdx.x].s[2] = v[0];
-  }
   __syncthreads();
   unsigned int* gh = LEVEL == 1 ? a.ws.hist1 : a.ws.hist2;
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
@@ -697,69 +714,175 @@ __global__ void __launch_bounds__(256) k_slot_gather(OpArgs a, int ns) {
   });
 }
 
-// Exact mass (and, for a rotation step, sum of |a|^4) of the children that
-// survive the selection: bits > T, or >= T when every child at T is kept; all
-// children when the op does not truncate.  Per-CTA partials s[0], s[1].
+// After a key tie-break: the tied children's slots become kSlotKeptTie (kept)
+// or 0 (dropped), so that the survivors are decided by the slot alone.
+__global__ void __launch_bounds__(256) k_tie_mark(OpArgs a, int ns) {
+  const SelState* sel = a.ws.sel;
+  if (!sel->tie || sel->stage != 3) return;
+  const long long m = sel->n_cand < a.ws.max_n ? sel->n_cand : a.ws.max_n;
+  const long long nslots = (long long)ns * a.in->nnz;
+  const unsigned long long tk = sel->t_key;
+  unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys);
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long i = a.ws.cand_bits[k];
+    if ((long long)i < nslots) slots[i] = (a.ws.cand_key[k] <= tk) ? kSlotKeptTie : 0ULL;
+  }
+}
+
+// One CTA per tile (block-strided over the tiles): the number of surviving
+// children of the tile (into ws.status[tile], for k_scan_tiles) and, per CTA
+// in partials s[0..2], the exact mass of the survivors, their sum of |a|^4
+// (rotation steps) and the exact mass of all children (truncating ops).  The
+// tile's slots are NS consecutive words per Z position of the tile.
 template <bool P2>
-__global__ void __launch_bounds__(256) k_slot_sums(OpArgs a, int ns) {
-  __shared__ i128 sRed[2 * 8];
-  __shared__ int sTrunc, sInclEq;
+__global__ void __launch_bounds__(256) k_tile_counts(OpArgs a, int ns, int kind) {
+  __shared__ i128 sRed[3 * 8];
+  __shared__ int sTrunc, sIncl, sCnt[8];
   __shared__ unsigned long long sT;
   if (threadIdx.x == 0) {
     const SelState* sel = a.ws.sel;
     sTrunc = sel->do_trunc;
-    sT = sel->t_bits;
-    sInclEq = sel->t_key == ~0ULL;
+    sT = sel->do_trunc ? sel->t_bits : 0ULL;
+    sIncl = !sel->do_trunc || sel->t_key == ~0ULL;
   }
   __syncthreads();
-  if (!P2 && !sTrunc) return;
-  const long long nslots = (long long)ns * a.in->nnz;
-  if (nslots > a.ws.max_n) return;
-  const unsigned long long T = sTrunc ? sT : 0ULL;
-  const bool incl = !sTrunc || sInclEq;
-  i128 v[2] = {0, 0};
-  scan_slots(reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys), nslots,
-             [&](unsigned long long bits, long long) {
-               if (bits != ~0ULL && (bits > T || (incl && bits == T))) {
-                 const double p = __longlong_as_double((long long)bits);
-                 v[0] += fx_from(p);
-                 if (P2) v[1] += fx_from(__dmul_rn(p, p));
-               }
-             });
-  block_sum_i128<2>(v, sRed);
-  if (threadIdx.x == 0) {
-    Partial* pt = a.ws.partials + blockIdx.x;
-    pt->s[0] = v[0];
-    pt->s[1] = v[1];
+  const long long n = a.in->nnz;
+  const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
+  const bool trunc = sTrunc;
+  const bool sums = P2 || trunc;
+  const unsigned long long T = sT;
+  const bool incl = sIncl;
+  i128 v[3] = {0, 0, 0};
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  const bool ok = ntiles <= a.ws.max_tiles && (long long)ns * n <= a.ws.max_n;
+  for (long long b = blockIdx.x; ok && b < ntiles; b += gridDim.x) {
+    long long z0, z1;
+    if (kind == K_IDENT) {
+      z0 = b * kTile;
+      z1 = (z0 + kTile < n) ? z0 + kTile : n;
+    } else {
+      z0 = a.ws.part[b * 6];
+      z1 = a.ws.part[(b + 1) * 6];
+    }
+    const long long s0 = ns * z0, s1 = ns * z1;
+    int cnt = 0;
+    for (long long i0 = s0; i0 < s1; i0 += 4 * 256) {
+      unsigned long long x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const long long i = i0 + u * 256 + threadIdx.x;
+        x[u] = (i < s1) ? slots[i] : ~0ULL;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool kept = slot_kept(x[u], T, incl);
+        cnt += kept;
+        if (sums && x[u] != ~0ULL && x[u] != kSlotKeptTie && x[u] != 0ULL) {
+          const double p = __longlong_as_double((long long)x[u]);
+          const i128 f = fx_from(p);
+          if (trunc) v[2] += f;
+          if (kept) {
+            v[0] += f;
+            if (P2) v[1] += fx_from(__dmul_rn(p, p));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    if (lane == 0) sCnt[w] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int c = 0;
+      for (int k = 0; k < 8; ++k) c += sCnt[k];
+      a.ws.status[b] = (unsigned long long)c;
+    }
+    __syncthreads();
+  }
+  if (sums) {
+    block_sum_i128<3>(v, sRed);
+    if (threadIdx.x == 0) {
+      Partial* pt = a.ws.partials + blockIdx.x;
+      pt->s[0] = v[0];
+      pt->s[1] = v[1];
+      pt->s[2] = v[2];
+    }
   }
 }
 
-// The kept mass (and sum of |a|^4) from k_slot_sums' partials; ties at T
+// Exclusive scan of the per-tile survivor counts (in place in ws.status):
+// every tile of the write pass then knows where its output starts.
+__global__ void __launch_bounds__(1024) k_scan_tiles(OpArgs a, int kind) {
+  __shared__ long long sW[32];
+  const long long n = a.in->nnz;
+  const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
+  if (ntiles > a.ws.max_tiles) return;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const long long per = (ntiles + blockDim.x - 1) / blockDim.x;
+  const long long b0 = t * per, b1 = (b0 + per < ntiles) ? b0 + per : ntiles;
+  long long run = 0;
+  for (long long b = b0; b < b1; ++b) run += (long long)a.ws.status[b];
+  long long x = run;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) sW[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    long long y = (lane < (int)(blockDim.x >> 5)) ? sW[lane] : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const long long z = __shfl_up_sync(0xffffffffu, y, off);
+      if (lane >= off) y += z;
+    }
+    sW[lane] = y;
+  }
+  __syncthreads();
+  long long ex = x - run + (w > 0 ? sW[w - 1] : 0);
+  for (long long b = b0; b < b1; ++b) {
+    const long long c = (long long)a.ws.status[b];
+    a.ws.status[b] = (unsigned long long)ex;
+    ex += c;
+  }
+  if (t == blockDim.x - 1) {
+    a.ws.sel->n_written = ex;
+    if (ex > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
+  }
+}
+
+// The kept mass (and sum of |a|^4) from k_tile_counts' partials; ties at T
 // settled by key contribute `need` copies of T.  mode 1 (rotation step, the
 // decision of bass_simulator.py:795-814): the candidate's PR = kept^2 /
 // sum |a|^4 against ctrl->pr_cur; a rejected candidate is not written unless
 // a trace is kept.
 __global__ void k_kept_final(OpArgs a, int nblk, int mode, int j, int trace) {
-  __shared__ i128 sRed[2 * 8];
+  __shared__ i128 sRed[3 * 8];
   SelState* sel = a.ws.sel;
   const int trunc = sel->do_trunc;
   if (mode == 0 && !trunc) return;
-  i128 v[2] = {0, 0};
+  i128 v[3] = {0, 0, 0};
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
     v[0] += a.ws.partials[b].s[0];
     v[1] += a.ws.partials[b].s[1];
+    v[2] += a.ws.partials[b].s[2];
   }
-  block_sum_i128<2>(v, sRed);
+  block_sum_i128<3>(v, sRed);
   if (threadIdx.x != 0) return;
-  if (trunc && sel->t_key != ~0ULL) {
+  if (trunc && sel->tie) {  // the tied children's slots were rewritten: add them back
     const double T = __longlong_as_double((long long)sel->t_bits);
-    v[0] += (i128)sel->need * fx_from(T);
+    const i128 f = fx_from(T);
+    v[0] += (i128)sel->need * f;
     v[1] += (i128)sel->need * fx_from(__dmul_rn(T, T));
+    v[2] += (i128)sel->n_cand * f;
   }
   const double kept = fx_to(v[0]);
   const double p2 = fx_to(v[1]);
   sel->kept = kept;
   sel->kept_p2 = p2;
+  if (trunc) sel->total = fx_to(v[2]);
   if (mode != 1) return;
   const long long n_kept = trunc ? (sel->k_keep > 0 ? sel->k_keep : 0) : sel->n_out;
   bass_ctrl* c = a.ctrl;
@@ -843,21 +966,22 @@ __device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, 
   return sRes;
 }
 
-// nblk: CTAs of the evaluation pass (child counts); nblk1: CTAs of the
-// level-1 slot histogram (exact mass of all children, when truncating).
-__global__ void __launch_bounds__(1024) k_select1(OpArgs a, int nblk, int nblk1) {
+// nblk: CTAs of the evaluation pass (per-CTA child counts).
+__global__ void __launch_bounds__(1024) k_select1(OpArgs a, int nblk) {
   __shared__ long long sS[1024];
-  __shared__ i128 sRed[2 * 32];
+  __shared__ long long sC[32];
   SelState* sel = a.ws.sel;
-  i128 v[2] = {0, 0};
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) v[1] += (i128)a.ws.partials[b].c[0];
-  for (int b = threadIdx.x; b < nblk1; b += blockDim.x) v[0] += a.ws.partials[b].s[2];
-  block_sum_i128<2>(v, sRed);
+  long long cn = 0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) cn += a.ws.partials[b].c[0];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) cn += __shfl_down_sync(0xffffffffu, cn, off);
+  if ((threadIdx.x & 31) == 0) sC[threadIdx.x >> 5] = cn;
+  __syncthreads();
   __shared__ int sGo;
   if (threadIdx.x == 0) {
-    const long long n_out = (long long)v[1];
+    long long n_out = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) n_out += sC[k];
     sel->n_out = n_out;
-    sel->total = fx_to(v[0]);  // meaningful only when the op truncates
     sel->k_keep = a.k_keep;
     sGo = 0;
     if (a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out) {
@@ -920,15 +1044,15 @@ __device__ __forceinline__ bool better(unsigned long long ab, unsigned long long
 }
 
 // Sorts the first m candidates by (bits desc, key asc) in shared memory
-// (m <= kCandSmem); block of 1024 threads.
+// (m <= kCandSmem); block of 1024 threads.  by_key_only: the candidates all
+// share one bit pattern and cand_bits holds their slot indices.
 __device__ void sort_candidates(unsigned long long* sb, unsigned long long* sk, long long m, const WsView& ws,
-                                bool keys_desc_by_bits_only) {
-  (void)keys_desc_by_bits_only;
+                                bool by_key_only) {
   const int tid = threadIdx.x;
   int P = 1;
   while (P < m) P <<= 1;
   for (int i = tid; i < P; i += blockDim.x) {
-    if (i < m) { sb[i] = ws.cand_bits[i]; sk[i] = ws.cand_key[i]; }
+    if (i < m) { sb[i] = by_key_only ? 1ULL : ws.cand_bits[i]; sk[i] = ws.cand_key[i]; }
     else { sb[i] = 0; sk[i] = ~0ULL; }
   }
   __syncthreads();
@@ -973,11 +1097,11 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
   __shared__ unsigned long long sT;
   __shared__ long long sGt, sEq;
   if (m <= kCandSmem) {
-    sort_candidates(sb, sk, m, a.ws, mode == 0);
+    sort_candidates(sb, sk, m, a.ws, mode == 1);
     if (tid == 0) {
       const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
       if (mode == 1) {
-        sel->t_bits = sb[r];
+        sel->t_bits = sel->prefix;
         sel->t_key = sk[r];
         sel->stage = 3;
       } else {
@@ -1071,6 +1195,7 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
       sel->stage = 3;
     } else {
       sel->stage = 4;
+      sel->tie = 1;
       sel->prefix = sT;
       sel->need = take;
       sel->n_cand = 0;
@@ -1205,7 +1330,7 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
     int gh = 0;
     if ((e = launch_tile<KIND, P_HIST>(a, 0, s, &gh)) != cudaSuccess) return e;
     KLAUNCH(S_SLOT_HIST1, s, k_slot_hist<1><<<gs, 256, 0, s>>>(a, ns, gh));
-    KLAUNCH(S_SELECT1, s, k_select1<<<1, 1024, 0, s>>>(a, gh, gs));
+    KLAUNCH(S_SELECT1, s, k_select1<<<1, 1024, 0, s>>>(a, gh));
     KLAUNCH(S_SLOT_HIST2, s, k_slot_hist<2><<<gs, 256, 0, s>>>(a, ns, gh));
     KLAUNCH(S_SELECT2, s, k_select2<<<1, 1024, 0, s>>>(a));
     KLAUNCH(S_SLOT_GATHER, s, k_slot_gather<<<gs, 256, 0, s>>>(a, ns));
@@ -1218,10 +1343,13 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
     KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a, 0));
     if ((e = launch_tile<KIND, P_GATHER>(a, 2, s, nullptr)) != cudaSuccess) return e;
     KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a, 1));
-    if (fin_mode == 1) KLAUNCH(S_SLOT_KEPT, s, k_slot_sums<true><<<gs, 256, 0, s>>>(a, ns));
-    else KLAUNCH(S_SLOT_KEPT, s, k_slot_sums<false><<<gs, 256, 0, s>>>(a, ns));
+    KLAUNCH(S_SLOT_KEPT, s, k_tie_mark<<<device().sms, 256, 0, s>>>(a, ns));
+    if (fin_mode == 1) KLAUNCH(S_SLOT_KEPT, s, k_tile_counts<true><<<gs, 256, 0, s>>>(a, ns, KIND));
+    else KLAUNCH(S_SLOT_KEPT, s, k_tile_counts<false><<<gs, 256, 0, s>>>(a, ns, KIND));
     KLAUNCH(S_REDUCE, s, k_kept_final<<<1, 256, 0, s>>>(a, gs, fin_mode, j, tr.trace));
+    KLAUNCH(S_REDUCE, s, k_scan_tiles<<<1, 1024, 0, s>>>(a, KIND));
   }
+  a.write_mode = (KIND == K_PERM) ? 2 : 1;
   int gw = 0;
   if ((e = launch_tile<KIND, P_WRITE>(a, 3, s, &gw)) != cudaSuccess) return e;
   KLAUNCH(S_FINALIZE, s, k_finalize<<<1, 32, 0, s>>>(a, tr, fin_mode, KIND));
@@ -1249,6 +1377,7 @@ cudaError_t run_commit(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const 
 // write pass only (keep everything the drop rule keeps); used by the guarded
 // compaction after a 1-qubit diagonal gate.  The caller zeroed the small region.
 cudaError_t run_ident_write(OpArgs a, cudaStream_t s) {
+  a.write_mode = 0;
   return launch_tile<K_IDENT, P_WRITE>(a, 3, s, nullptr);
 }
 
