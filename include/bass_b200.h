@@ -68,7 +68,8 @@ typedef struct bass_state {
    1 hist2, 2 gather, 3 write, 4 rdm), then 30 partition, 31 select1,
    32 select2, 33 select_exact, 34 finalize, 35 reductions, 36 fingerprint,
    37 phase2q, 38 phase1q, 39 rdm_final, 40 radix sort, 41 merge runs,
-   42 small bookkeeping kernels. */
+   42 small bookkeeping kernels, 43 / 44 level-1 / level-2 slot histograms,
+   45 slot gather, 46 tie marking and per-tile survivor counts. */
 #define BASS_PROF_SLOTS 48
 
 typedef struct bass_ctrl {
