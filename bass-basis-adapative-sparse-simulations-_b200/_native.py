@@ -41,7 +41,7 @@ PROF_SLOTS = 48
 KINDS = ["gate1", "rot1", "gate2", "perm", "plain", "rdm"]
 PASSES = ["hist", "hist2", "gather", "write", "rdm"]
 SLOT_NAMES = [f"k_tile<{k},{p}>" for k in KINDS for p in PASSES] + [
-    "k_partition", "k_select1", "k_select2", "k_select_exact", "k_finalize", "reductions", "k_fingerprint",
+    "k_partition", "k_select_coop", "k_select2", "k_tie_coop", "k_finalize", "reductions", "k_fingerprint",
     "k_phase2q", "k_phase1q", "k_rdm_final", "radix_sort", "merge_runs", "bookkeeping", "k_slot_hist<1>",
     "k_slot_hist<2>", "k_slot_gather", "k_tile_counts"] + [f"slot{i}" for i in range(47, 48)]
 

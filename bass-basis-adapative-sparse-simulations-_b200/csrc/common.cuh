@@ -62,6 +62,17 @@ __host__ __device__ __forceinline__ i128 fx_from_bits(double v) {
   return (b >> 63) ? -r : r;
 }
 
+// fx_from of a non-negative finite double given by its bit pattern (a
+// probability), with integer operations only.
+__device__ __forceinline__ i128 fx_from_pbits(unsigned long long b) {
+  const int e = (int)(b >> 52);
+  const unsigned long long m = (b & 0xFFFFFFFFFFFFFULL) | 0x10000000000000ULL;
+  const int sh = e - 1075 + kFxFrac;  // value * 2^96 = m * 2^sh
+  if (e == 0 || sh <= -64) return 0;
+  if (sh < 0) return (i128)(m >> (-sh));
+  return (i128)((u128)m << sh);
+}
+
 // On the device, for |v| < 2^31 (every probability and moment summed here),
 // the same integer is formed in exact floating-point steps: hi =
 // floor(|v| * 2^32) and lo = floor(frac(|v| * 2^32) * 2^64); both scalings are

@@ -20,8 +20,9 @@
 //   k_select*     radix select of the top-k threshold (13-bit digits on the
 //                 IEEE bits of |a|^2, then an exact (|a|^2 desc, key asc)
 //                 ordering of the boundary candidates);
-//   k_finalize    output descriptor (count, new bit order, pending
-//                 renormalisation) and the gamma / truncation bookkeeping.
+//   finalize_op   (last CTA of the write pass) output descriptor (count, new
+//                 bit order, pending renormalisation) and the gamma /
+//                 truncation bookkeeping.
 //
 // The output is again sorted by its (new) physical key: children of a group
 // are emitted in child-index order, groups in Z order.
@@ -227,13 +228,76 @@ constexpr unsigned long long kSlotKeptTie = 0x7FFFFFFFFFFFFFFEULL;
 
 // Does the child with this slot survive the selection?  (T, incl) = (t_bits,
 // t_key == ~0) when truncating, (0, true) otherwise; ties settled by key were
-// rewritten to kSlotKeptTie / 0 by k_tie_mark.
+// rewritten to kSlotKeptTie / 0 by k_tie_coop.
 __device__ __forceinline__ bool slot_kept(unsigned long long bits, unsigned long long T, bool incl) {
   return bits != ~0ULL && (bits > T || (incl && bits == T));
 }
 
 __host__ __device__ constexpr int slots_per_entry(int kind) {
   return kind == K_GATE2 ? 4 : (kind == K_GATE1 || kind == K_ROT1) ? 2 : 1;
+}
+
+// ---------------------------------------------------------------------------
+// finalisation
+// ---------------------------------------------------------------------------
+// mode 0: plain op; mode 1: basis-rotation step (always renormalises, keeps
+// the retained mass in sel->kept for the decision)
+// The kept mass comes from the selection's final phase (set when the op
+// truncates or is a rotation step, the only cases that use it).
+// One thread.  Runs in the last CTA of the write pass to finish, so the
+// selection's results (written by the previous kernel) and n_written (written
+// by the CTA of the last tile, before its fence) are read through volatile.
+__device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int kind) {
+  volatile SelState* sel = a.ws.sel;
+  const bass_state* in = a.in;
+  bass_state* out = a.out;
+  bass_ctrl* c = a.ctrl;
+  const double kept = sel->kept;
+  const long long n_in = in->nnz;
+  long long nw = sel->n_written;
+  if (nw > out->cap) {  // the write pass skipped the tiles that did not fit
+    set_error(c, BASS_ERR_CAPACITY);
+    nw = 0;
+  }
+  const int t = (kind == K_IDENT) ? 0 : in->pos[a.q];
+  int8_t qat[64];
+  out_order(in, kind, t, a.gb, qat);
+  for (int p = 0; p < 64; ++p) {
+    out->qat[p] = qat[p];
+    out->pos[qat[p]] = (int8_t)p;
+  }
+  out->nq = in->nq;
+  out->nnz = nw;
+  out->rscale[0] = 1.0;
+  out->rscale[1] = 1.0;
+  if (kind == K_PERM) return;  // first pass of a 2-qubit gate: no bookkeeping
+  c->amp_updates += n_in;
+  c->n_ops += 1;
+  const int trunc = sel->do_trunc;
+  if (mode == 1) {
+    const double nrm = sqrt(kept);
+    if (nrm > 1e-30) out->rscale[0] = 1.0 / nrm;
+    return;
+  }
+  c->last_truncated = trunc;
+  if (!trunc) return;
+  const double total = sel->total;
+  c->last_kept = kept;
+  c->last_total = total;
+  c->n_trunc += 1;
+  if (tr.gamma_mode == 1) c->gamma_running *= (total > 1e-30 ? kept / total : 0.0);
+  else if (tr.gamma_mode == 2) c->state_gamma *= (total > 1e-30 ? sqrt(kept / total) : 0.0);
+  else if (tr.gamma_mode == 3) c->state_gamma *= sqrt(kept);
+  if (tr.renorm == 1) {
+    const double nrm = sqrt(kept);
+    if (nrm > 1e-30) out->rscale[0] = 1.0 / nrm;
+  } else if (tr.renorm == 2) {
+    out->rscale[0] = 1.0 / sqrt(kept);
+  }
+  if (tr.mark_active) {
+    c->truncation_active = 1;
+    c->gates_since_trunc = 0;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -264,8 +328,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
   if (tid == 0) S = *a.ws.sel;
   __syncthreads();
   if (PASS == P_GATHER && S.stage != 4) return;
-  if (PASS == P_WRITE && S.skip_write) return;
   if (KIND == K_IDENT && a.guard && S.pad == 0) return;
+  // a rejected rotation candidate is not written (the descriptor still is)
+  const bool skip = PASS == P_WRITE && S.skip_write;
 
   if (tid == 0) {
     const bass_state* in = a.in;
@@ -284,12 +349,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
   const int gb = a.gb;
   const long long ntiles = H.ntiles;
   constexpr int NS = slots_per_entry(KIND);
-  if (ntiles > a.ws.max_tiles || (PASS == P_HIST && (long long)NS * H.n > a.ws.max_n)) {
-    if (blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
-    return;
-  }
+  const bool bad = ntiles > a.ws.max_tiles || (PASS == P_HIST && (long long)NS * H.n > a.ws.max_n);
+  if (bad && blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+  if (bad && PASS != P_WRITE) return;
   const bool scaled = !(H.r0 == 1.0 && H.r1 == 1.0);
-  const long long nitems = (KIND == K_RDM) ? ntiles * a.nsets : ntiles;
+  const long long nitems = (bad || skip) ? 0 : (KIND == K_RDM) ? ntiles * a.nsets : ntiles;
   long long cnt = 0;
   const int base_e = tid * kPerThread;
 
@@ -489,7 +553,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
       }
     } else if (PASS == P_WRITE) {
       // write_mode 1: kept children from the slot array, tile base from
-      //   k_scan_tiles; 2: one child per entry, base = the tile's Z start;
+      //   the selection's tile scan; 2: one child per entry, base = the tile's Z start;
       //   0: the drop rule decides, base by decoupled look-back.
       constexpr int MC = KindTraits<KIND>::kMaxChildren;
       uint64_t kb;
@@ -630,6 +694,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
     __syncthreads();
   }
 
+  // ---- write pass: the last CTA to finish writes the output descriptor ------
+  if (PASS == P_WRITE && a.fin) {
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      const unsigned long long d =
+          atomicAdd(&reinterpret_cast<unsigned long long*>(a.ws.counters)[59], 1ULL);
+      if (d == gridDim.x - 1) {
+        __threadfence();
+        finalize_op(a, a.tr, a.fin_mode, KIND);
+      }
+    }
+  }
+
   // ---- flush: the CTA's child count ----------------------------------------
   if (PASS == P_HIST) {
 #pragma unroll
@@ -645,315 +723,95 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// streaming passes over the slot array (one |a|^2 bit pattern per child,
-// ~0 where a group has fewer children than slots)
+// selection: one cooperative launch per op
 // ---------------------------------------------------------------------------
-// LEVEL 1: histogram of bits >> 50 over all slots, only when the op
-// truncates (count from the evaluation pass's per-CTA partials); LEVEL 2:
-// bits 37-49 of the slots inside the level-1 boundary bin.
-template <int LEVEL>
-__global__ void __launch_bounds__(256) k_slot_hist(OpArgs a, int ns, int nblk) {
-  __shared__ unsigned int h[kHistBins];
-  __shared__ int sGo;
-  __shared__ unsigned long long sPrefix;
-  __shared__ long long sCnt[8];
-  if (LEVEL == 1) {
-    long long c = 0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) c += a.ws.partials[b].c[0];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
-    if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      long long n_out = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) n_out += sCnt[w];
-      sGo = !(a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out);
-      sPrefix = 0;
-    }
-  } else if (threadIdx.x == 0) {
-    sGo = a.ws.sel->stage == 1;
-    sPrefix = a.ws.sel->prefix;
-  }
-  __syncthreads();
-  if (!sGo) return;
-  for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) h[i] = 0;
-  __syncthreads();
-  const long long nslots = (long long)ns * a.in->nnz;
-  if (nslots > a.ws.max_n) return;
-  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
-  const unsigned long long pre = sPrefix;
-  scan_slots(slots, nslots, [&](unsigned long long bits, long long) {
-    const bool valid = bits != ~0ULL && (LEVEL == 1 || (bits >> 50) == pre);
-    const unsigned bin = LEVEL == 1 ? (unsigned)(bits >> 50) : (unsigned)((bits >> 37) & (kHistBins - 1));
-    hist_add(h, bin, valid);
-  });
-  __syncthreads();
-  unsigned int* gh = LEVEL == 1 ? a.ws.hist1 : a.ws.hist2;
-  for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
-    if (h[i]) atomicAdd(&gh[i], h[i]);
-}
+// After the evaluation pass has written every child's |a|^2 bit pattern to the
+// slot array (NS words per Z position, ~0 where a group has fewer children),
+// k_select_coop finds the top-k threshold and prepares the write pass:
+//   1. the child count (from the evaluation pass's per-CTA partials) decides
+//      whether the op truncates;
+//   2. radix select on the bit patterns: a 13-bit histogram of bits 50-62,
+//      then of bits 37-49 inside the boundary bin, then the exact candidates
+//      of the boundary bin (block 0); every block reads the histograms and
+//      finds the boundary bins itself, so each level costs one grid barrier;
+//   3. per tile, the number of survivors (into ws.status) and per CTA the
+//      exact kept mass, total mass and, for a rotation step, sum of |a|^4;
+//   4. block 0: the exact sums, the rotation decision, and an exclusive scan
+//      of the tile counts (each tile of the write pass then knows its base).
+// An exact tie at the threshold (equal bit patterns straddling rank k) stops
+// it after step 2; the tied children's keys are then collected by the tile
+// kernel's P_GATHER pass and k_tie_coop settles the tie by key and runs
+// steps 3-4.  The grid barrier is a counter and a generation word in the
+// workspace with a bounded spin (BASS_ERR_WAIT, then every block returns).
+constexpr int kSelThreads = 512;
 
-// candidates of the level-2 boundary bin: (bits, slot index)
-__global__ void __launch_bounds__(256) k_slot_gather(OpArgs a, int ns) {
-  SelState* sel = a.ws.sel;
-  if (sel->stage != 2) return;
-  const unsigned long long pre = sel->prefix;
-  const long long nslots = (long long)ns * a.in->nnz;
-  if (nslots > a.ws.max_n) return;
-  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
-  scan_slots(slots, nslots, [&](unsigned long long bits, long long i) {
-    if (bits != ~0ULL && (bits >> 37) == pre) {
-      const unsigned long long k = atomicAdd(reinterpret_cast<unsigned long long*>(&sel->n_cand), 1ULL);
-      if ((long long)k < a.ws.max_n) {
-        a.ws.cand_bits[k] = bits;
-        a.ws.cand_key[k] = (unsigned long long)i;
-      } else {
-        sel->cand_overflow = 1;
-      }
-    }
-  });
-}
-
-// After a key tie-break: the tied children's slots become kSlotKeptTie (kept)
-// or 0 (dropped), so that the survivors are decided by the slot alone.
-__global__ void __launch_bounds__(256) k_tie_mark(OpArgs a, int ns) {
-  const SelState* sel = a.ws.sel;
-  if (!sel->tie || sel->stage != 3) return;
-  const long long m = sel->n_cand < a.ws.max_n ? sel->n_cand : a.ws.max_n;
-  const long long nslots = (long long)ns * a.in->nnz;
-  const unsigned long long tk = sel->t_key;
-  unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys);
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x) {
-    const unsigned long long i = a.ws.cand_bits[k];
-    if ((long long)i < nslots) slots[i] = (a.ws.cand_key[k] <= tk) ? kSlotKeptTie : 0ULL;
-  }
-}
-
-// One CTA per tile (block-strided over the tiles): the number of surviving
-// children of the tile (into ws.status[tile], for k_scan_tiles) and, per CTA
-// in partials s[0..2], the exact mass of the survivors, their sum of |a|^4
-// (rotation steps) and the exact mass of all children (truncating ops).  The
-// tile's slots are NS consecutive words per Z position of the tile.
-template <bool P2>
-__global__ void __launch_bounds__(256) k_tile_counts(OpArgs a, int ns, int kind) {
-  __shared__ i128 sRed[3 * 8];
-  __shared__ int sTrunc, sIncl, sCnt[8];
-  __shared__ unsigned long long sT;
+// Grid-wide barrier of a cooperative launch.  Returns false (error recorded)
+// if the wait gave up.
+__device__ bool grid_sync(const OpArgs& a) {
+  __shared__ int sOk;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    const SelState* sel = a.ws.sel;
-    sTrunc = sel->do_trunc;
-    sT = sel->do_trunc ? sel->t_bits : 0ULL;
-    sIncl = !sel->do_trunc || sel->t_key == ~0ULL;
-  }
-  __syncthreads();
-  const long long n = a.in->nnz;
-  const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
-  const bool trunc = sTrunc;
-  const bool sums = P2 || trunc;
-  const unsigned long long T = sT;
-  const bool incl = sIncl;
-  i128 v[3] = {0, 0, 0};
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
-  const bool ok = ntiles <= a.ws.max_tiles && (long long)ns * n <= a.ws.max_n;
-  for (long long b = blockIdx.x; ok && b < ntiles; b += gridDim.x) {
-    long long z0, z1;
-    if (kind == K_IDENT) {
-      z0 = b * kTile;
-      z1 = (z0 + kTile < n) ? z0 + kTile : n;
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(a.ws.counters) + 60;
+    unsigned long long* gen = cnt + 1;
+    const unsigned long long g = ld_acquire(gen);
+    __threadfence();
+    const unsigned long long arrived = atomicAdd(cnt, 1ULL);
+    int ok = 1;
+    if (arrived == gridDim.x - 1) {
+      atomicExch(cnt, 0ULL);
+      __threadfence();
+      st_release(gen, g + 1);
     } else {
-      z0 = a.ws.part[b * 6];
-      z1 = a.ws.part[(b + 1) * 6];
-    }
-    const long long s0 = ns * z0, s1 = ns * z1;
-    int cnt = 0;
-    for (long long i0 = s0; i0 < s1; i0 += 4 * 256) {
-      unsigned long long x[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const long long i = i0 + u * 256 + threadIdx.x;
-        x[u] = (i < s1) ? slots[i] : ~0ULL;
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const bool kept = slot_kept(x[u], T, incl);
-        cnt += kept;
-        if (sums && x[u] != ~0ULL && x[u] != kSlotKeptTie && x[u] != 0ULL) {
-          const double p = __longlong_as_double((long long)x[u]);
-          const i128 f = fx_from(p);
-          if (trunc) v[2] += f;
-          if (kept) {
-            v[0] += f;
-            if (P2) v[1] += fx_from(__dmul_rn(p, p));
-          }
+      long long spins = 0;
+      while (ld_acquire(gen) == g) {
+        if (++spins > kSpinLimit) {
+          set_error(a.ctrl, BASS_ERR_WAIT);
+          ok = 0;
+          break;
         }
       }
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
-    if (lane == 0) sCnt[w] = cnt;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int c = 0;
-      for (int k = 0; k < 8; ++k) c += sCnt[k];
-      a.ws.status[b] = (unsigned long long)c;
-    }
-    __syncthreads();
-  }
-  if (sums) {
-    block_sum_i128<3>(v, sRed);
-    if (threadIdx.x == 0) {
-      Partial* pt = a.ws.partials + blockIdx.x;
-      pt->s[0] = v[0];
-      pt->s[1] = v[1];
-      pt->s[2] = v[2];
-    }
-  }
-}
-
-// Exclusive scan of the per-tile survivor counts (in place in ws.status):
-// every tile of the write pass then knows where its output starts.
-__global__ void __launch_bounds__(1024) k_scan_tiles(OpArgs a, int kind) {
-  __shared__ long long sW[32];
-  const long long n = a.in->nnz;
-  const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
-  if (ntiles > a.ws.max_tiles) return;
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const long long per = (ntiles + blockDim.x - 1) / blockDim.x;
-  const long long b0 = t * per, b1 = (b0 + per < ntiles) ? b0 + per : ntiles;
-  long long run = 0;
-  for (long long b = b0; b < b1; ++b) run += (long long)a.ws.status[b];
-  long long x = run;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const long long y = __shfl_up_sync(0xffffffffu, x, off);
-    if (lane >= off) x += y;
-  }
-  if (lane == 31) sW[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    long long y = (lane < (int)(blockDim.x >> 5)) ? sW[lane] : 0;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const long long z = __shfl_up_sync(0xffffffffu, y, off);
-      if (lane >= off) y += z;
-    }
-    sW[lane] = y;
+    __threadfence();
+    sOk = ok;
   }
   __syncthreads();
-  long long ex = x - run + (w > 0 ? sW[w - 1] : 0);
-  for (long long b = b0; b < b1; ++b) {
-    const long long c = (long long)a.ws.status[b];
-    a.ws.status[b] = (unsigned long long)ex;
-    ex += c;
-  }
-  if (t == blockDim.x - 1) {
-    a.ws.sel->n_written = ex;
-    if (ex > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
-  }
+  return sOk != 0;
 }
 
-// The kept mass (and sum of |a|^4) from k_tile_counts' partials; ties at T
-// settled by key contribute `need` copies of T.  mode 1 (rotation step, the
-// decision of bass_simulator.py:795-814): the candidate's PR = kept^2 /
-// sum |a|^4 against ctrl->pr_cur; a rejected candidate is not written unless
-// a trace is kept.
-__global__ void k_kept_final(OpArgs a, int nblk, int mode, int j, int trace) {
-  __shared__ i128 sRed[3 * 8];
-  SelState* sel = a.ws.sel;
-  const int trunc = sel->do_trunc;
-  if (mode == 0 && !trunc) return;
-  i128 v[3] = {0, 0, 0};
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-    v[0] += a.ws.partials[b].s[0];
-    v[1] += a.ws.partials[b].s[1];
-    v[2] += a.ws.partials[b].s[2];
-  }
-  block_sum_i128<3>(v, sRed);
-  if (threadIdx.x != 0) return;
-  if (trunc && sel->tie) {  // the tied children's slots were rewritten: add them back
-    const double T = __longlong_as_double((long long)sel->t_bits);
-    const i128 f = fx_from(T);
-    v[0] += (i128)sel->need * f;
-    v[1] += (i128)sel->need * fx_from(__dmul_rn(T, T));
-    v[2] += (i128)sel->n_cand * f;
-  }
-  const double kept = fx_to(v[0]);
-  const double p2 = fx_to(v[1]);
-  sel->kept = kept;
-  sel->kept_p2 = p2;
-  if (trunc) sel->total = fx_to(v[2]);
-  if (mode != 1) return;
-  const long long n_kept = trunc ? (sel->k_keep > 0 ? sel->k_keep : 0) : sel->n_out;
-  bass_ctrl* c = a.ctrl;
-  const double pr_new = (n_kept == 0 || !(p2 > 0.0)) ? INFINITY : __ddiv_rn(__dmul_rn(kept, kept), p2);
-  const bool reject = pr_new >= c->pr_cur * (1.0 - c->pr_tie_tol);
-  c->frac[j] = kept;
-  c->accept[j] = reject ? 0 : 1;
-  sel->accept = reject ? 0 : 1;
-  sel->pr_new = pr_new;
-  sel->skip_write = (reject && !trace) ? 1 : 0;
-}
-
-// Rotation step, after the write pass: keep the candidate if accepted.
-__global__ void k_commit(bass_state* cur, bass_state* tmp, WsView ws, bass_ctrl* c, int j, int trace) {
-  const SelState* sel = ws.sel;
-  if (!sel->accept) return;
-  bass_state t = *cur;
-  *cur = *tmp;
-  *tmp = t;
-  c->pr_cur = sel->pr_new;
-  const double frac = c->frac[j];
-  c->gamma_running *= sqrt(frac > 1e-30 ? frac : 0.0);
-  if (trace && c->trace) {
-    const long long i = c->trace_len;
-    if (i >= c->trace_cap) {
-      set_error(c, BASS_ERR_CAPACITY);
-      return;
-    }
-    uint64_t* e = c->trace + i * BASS_TRACE_WORDS;
-    e[0] = 1;
-    e[1] = (uint64_t)j;
-    for (int k = 2; k < BASS_TRACE_WORDS; ++k) e[k] = 0;
-    c->trace_len = i + 1;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// selection
-// ---------------------------------------------------------------------------
-// Block of 1024 threads.  Returns the bin b with count(bins > b) < k <=
-// count(bins >= b); *c_gt = count(bins > b).  Needs 1 <= k <= total.
+// Block-wide: the bin b of an 8192-bin histogram (in global memory, written by
+// other blocks) with count(bins > b) < k <= count(bins >= b); *c_gt =
+// count(bins > b).  Needs 1 <= k <= total and blockDim.x dividing 8192.
 __device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, long long* sS) {
   __shared__ int sRes;
   __shared__ long long sAbove;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int per = kHistBins / nt;   // bins per thread
+  const int lanes_per = nt / 32;    // sS entries per lane of warp 0
   long long s = 0;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) s += hist[8 * t + i];
+  for (int i = 0; i < per; ++i) s += __ldcg(hist + per * t + i);
   sS[t] = s;
   __syncthreads();
   if (t < 32) {
     long long ls = 0;
-    for (int i = 0; i < 32; ++i) ls += sS[32 * t + i];
+    for (int i = 0; i < lanes_per; ++i) ls += sS[lanes_per * t + i];
     long long suf = ls;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      long long v = __shfl_down_sync(0xffffffffu, suf, off);
+      const long long v = __shfl_down_sync(0xffffffffu, suf, off);
       if (t + off < 32) suf += v;
     }
     const unsigned m = __ballot_sync(0xffffffffu, suf >= k);
     const int L = m ? 31 - __clz(m) : 0;
     if (t == L) {
       long long above = suf - ls;
-      int tt = 32 * L + 31;
-      for (; tt > 32 * L; --tt) {
+      int tt = lanes_per * L + lanes_per - 1;
+      for (; tt > lanes_per * L; --tt) {
         if (above + sS[tt] >= k) break;
         above += sS[tt];
       }
-      int b = 8 * tt + 7;
-      for (; b > 8 * tt; --b) {
-        const long long h = hist[b];
+      int b = per * tt + per - 1;
+      for (; b > per * tt; --b) {
+        const long long h = __ldcg(hist + b);
         if (above + h >= k) break;
         above += h;
       }
@@ -966,75 +824,46 @@ __device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, 
   return sRes;
 }
 
-// nblk: CTAs of the evaluation pass (per-CTA child counts).
-__global__ void __launch_bounds__(1024) k_select1(OpArgs a, int nblk) {
-  __shared__ long long sS[1024];
-  __shared__ long long sC[32];
-  SelState* sel = a.ws.sel;
-  long long cn = 0;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) cn += a.ws.partials[b].c[0];
+// Block-wide histogram of the slots (LEVEL 1: bits >> 50; LEVEL 2: bits
+// 37-49 of the slots whose bits >> 50 equal pre), added into gh.
+template <int LEVEL>
+__device__ void slot_hist_phase(const unsigned long long* slots, long long nslots, unsigned long long pre,
+                                unsigned int* h, unsigned int* gh) {
+  for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  // eight slots per thread and round, plain shared atomics (measured faster
+  // here than warp aggregation with __match_any_sync)
+  const ulonglong2* v = reinterpret_cast<const ulonglong2*>(slots);
+  const long long n2 = nslots >> 1;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long b = (long long)blockIdx.x * blockDim.x; b < n2; b += 4 * stride) {
+    unsigned key[8];
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) cn += __shfl_down_sync(0xffffffffu, cn, off);
-  if ((threadIdx.x & 31) == 0) sC[threadIdx.x >> 5] = cn;
-  __syncthreads();
-  __shared__ int sGo;
-  if (threadIdx.x == 0) {
-    long long n_out = 0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) n_out += sC[k];
-    sel->n_out = n_out;
-    sel->k_keep = a.k_keep;
-    sGo = 0;
-    if (a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out) {
-      sel->do_trunc = 0;
-      sel->stage = 0;
-    } else if (a.k_keep <= 0) {
-      sel->do_trunc = 1;
-      sel->stage = 3;
-      sel->t_bits = ~0ULL;
-      sel->t_key = 0;
-    } else {
-      sel->do_trunc = 1;
-      sGo = 1;
+    for (int u = 0; u < 4; ++u) {
+      const long long i = b + u * stride + threadIdx.x;
+      const ulonglong2 x = (i < n2) ? v[i] : make_ulonglong2(~0ULL, ~0ULL);
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const unsigned long long bits = c ? x.y : x.x;
+        const bool valid = bits != ~0ULL && (LEVEL == 1 || (bits >> 50) == pre);
+        const unsigned bin =
+            LEVEL == 1 ? (unsigned)(bits >> 50) : (unsigned)((bits >> 37) & (kHistBins - 1));
+        key[2 * u + c] = valid ? bin : 0xFFFFFFFFu;
+      }
     }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (key[u] != 0xFFFFFFFFu) atomicAdd(&h[key[u]], 1u);
+  }
+  if ((nslots & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long bits = slots[nslots - 1];
+    const bool valid = bits != ~0ULL && (LEVEL == 1 || (bits >> 50) == pre);
+    const unsigned bin = LEVEL == 1 ? (unsigned)(bits >> 50) : (unsigned)((bits >> 37) & (kHistBins - 1));
+    if (valid) atomicAdd(&h[bin], 1u);
   }
   __syncthreads();
-  if (!sGo) return;
-  long long c_gt;
-  const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, sS);
-  if (threadIdx.x == 0) {
-    const long long need = a.k_keep - c_gt;
-    if ((long long)a.ws.hist1[b1] == need) {
-      sel->stage = 3;
-      sel->t_bits = (unsigned long long)b1 << 50;
-      sel->t_key = ~0ULL;
-    } else {
-      sel->stage = 1;
-      sel->prefix = (unsigned long long)b1;
-      sel->need = need;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(1024) k_select2(OpArgs a) {
-  __shared__ long long sS[1024];
-  SelState* sel = a.ws.sel;
-  if (sel->stage != 1) return;
-  long long c_gt;
-  const long long need = sel->need;
-  const int b2 = find_bin(a.ws.hist2, need, &c_gt, sS);
-  if (threadIdx.x == 0) {
-    const long long need2 = need - c_gt;
-    const unsigned long long pre = (sel->prefix << 13) | (unsigned long long)b2;
-    if ((long long)a.ws.hist2[b2] == need2) {
-      sel->stage = 3;
-      sel->t_bits = pre << 37;
-      sel->t_key = ~0ULL;
-    } else {
-      sel->stage = 2;
-      sel->prefix = pre;
-      sel->need = need2;
-    }
-  }
+  for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
+    if (h[i]) atomicAdd(&gh[i], h[i]);
 }
 
 // better(a, b): a ranks strictly above b
@@ -1044,16 +873,21 @@ __device__ __forceinline__ bool better(unsigned long long ab, unsigned long long
 }
 
 // Sorts the first m candidates by (bits desc, key asc) in shared memory
-// (m <= kCandSmem); block of 1024 threads.  by_key_only: the candidates all
-// share one bit pattern and cand_bits holds their slot indices.
+// (m <= kCandSmem).  by_key_only: the candidates all share one bit pattern
+// and cand_bits holds their slot indices.
 __device__ void sort_candidates(unsigned long long* sb, unsigned long long* sk, long long m, const WsView& ws,
                                 bool by_key_only) {
   const int tid = threadIdx.x;
   int P = 1;
   while (P < m) P <<= 1;
   for (int i = tid; i < P; i += blockDim.x) {
-    if (i < m) { sb[i] = by_key_only ? 1ULL : ws.cand_bits[i]; sk[i] = ws.cand_key[i]; }
-    else { sb[i] = 0; sk[i] = ~0ULL; }
+    if (i < m) {
+      sb[i] = by_key_only ? 1ULL : __ldcg(ws.cand_bits + i);
+      sk[i] = __ldcg(ws.cand_key + i);
+    } else {
+      sb[i] = 0;
+      sk[i] = ~0ULL;
+    }
   }
   __syncthreads();
   for (int size = 2; size <= P; size <<= 1) {
@@ -1074,25 +908,31 @@ __device__ void sort_candidates(unsigned long long* sb, unsigned long long* sk, 
   }
 }
 
-// mode 0 (after the slot gather, stage 2): candidates are (bits, slot) of the
-//   level-2 boundary bin; find the need-th largest bit pattern T.  If every
-//   candidate equal to T is needed the threshold is resolved (keep bits >= T);
-//   otherwise the tie is settled by true key (stage 4: collect the tied
-//   children with their keys).
-// mode 1 (after the key pass, stage 4): candidates are (T, true key); keep the
-//   need smallest keys.
-__global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// One block.  mode 0 (stage 2): candidates are (bits, slot) of the level-2
+//   boundary bin; find the need-th largest bit pattern T.  If every candidate
+//   equal to T is needed the threshold is resolved (keep bits >= T, stage 3);
+//   otherwise the tie is settled by true key (stage 4: the tied children are
+//   collected with their keys).
+// mode 1 (stage 4): candidates are (slot, true key) of the children at T;
+//   keep the need smallest keys (stage 3 with t_key).
+__device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem) {
   unsigned long long* sb = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* sk = sb + kCandSmem;
   SelState* sel = a.ws.sel;
-  if (sel->stage != (mode == 0 ? 2 : 4)) return;
-  long long m = sel->n_cand;
-  if (sel->cand_overflow || m > a.ws.max_n) {
-    if (threadIdx.x == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
-    m = a.ws.max_n;
+  __shared__ long long sM, sNeedIn;
+  __shared__ unsigned long long sPre;
+  if (threadIdx.x == 0) {
+    long long m = *(volatile long long*)&sel->n_cand;
+    if (*(volatile int*)&sel->cand_overflow || m > a.ws.max_n) {
+      set_error(a.ctrl, BASS_ERR_WORKSPACE);
+      m = a.ws.max_n;
+    }
+    sM = m;
+    sNeedIn = sel->need;
+    sPre = sel->prefix;
   }
-  const long long need = sel->need;
+  __syncthreads();
+  const long long m = sM, need = sNeedIn;
   const int tid = threadIdx.x;
   __shared__ unsigned long long sT;
   __shared__ long long sGt, sEq;
@@ -1101,7 +941,7 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
     if (tid == 0) {
       const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
       if (mode == 1) {
-        sel->t_bits = sel->prefix;
+        sel->t_bits = sPre;
         sel->t_key = sk[r];
         sel->stage = 3;
       } else {
@@ -1126,7 +966,7 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
       __syncthreads();
       const unsigned long long pre = sKeyPre;
       for (long long i = tid; i < m; i += blockDim.x) {
-        const unsigned long long k = a.ws.cand_key[i];
+        const unsigned long long k = __ldcg(a.ws.cand_key + i);
         if (shift == 56 || (k >> (shift + 8)) == pre) atomicAdd(&h[(unsigned)(k >> shift) & 255u], 1u);
       }
       __syncthreads();
@@ -1143,10 +983,11 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
       __syncthreads();
     }
     if (tid == 0) {
-      sel->t_bits = sel->prefix;
+      sel->t_bits = sPre;
       sel->t_key = sKeyPre;
       sel->stage = 3;
     }
+    __syncthreads();
     return;
   } else {
     // many candidates: radix select on the low 37 bits of the bit pattern
@@ -1162,7 +1003,7 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
       __syncthreads();
       const unsigned long long pre = sLow;
       for (long long i = tid; i < m; i += blockDim.x) {
-        const unsigned long long lb = a.ws.cand_bits[i] & m37;
+        const unsigned long long lb = __ldcg(a.ws.cand_bits + i) & m37;
         if (shift == 32 || (lb >> (shift + 8)) == pre) atomicAdd(&h[(unsigned)(lb >> shift) & 255u], 1u);
       }
       __syncthreads();
@@ -1180,8 +1021,7 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
       __syncthreads();
     }
     if (tid == 0) {
-      const unsigned long long T = (sel->prefix << 37) | sLow;
-      sT = T;
+      sT = (sPre << 37) | sLow;
       sGt = need - sNeed;
       sEq = sLastCount;
     }
@@ -1202,66 +1042,343 @@ __global__ void __launch_bounds__(1024) k_select_exact(OpArgs a, int mode) {
       sel->cand_overflow = 0;
     }
   }
+  __syncthreads();
 }
 
-// ---------------------------------------------------------------------------
-// finalisation
-// ---------------------------------------------------------------------------
-// mode 0: plain op; mode 1: basis-rotation step (always renormalises, keeps
-// the retained mass in sel->kept for the decision)
-// The kept mass comes from k_kept_final (set when the op truncates or is a
-// rotation step, the only cases that use it).
-__global__ void k_finalize(OpArgs a, bass_trunc tr, int mode, int kind) {
+// The tile holding Z position z (tiles start at the partition's adjusted
+// positions P'_b <= b * kStep; plain tiles every kTile positions).
+__device__ __forceinline__ long long tile_of(long long z, int kind, const long long* part) {
+  if (kind == K_IDENT) return z / kTile;
+  const long long b0 = z / kStep;
+  return (z >= part[(b0 + 1) * 6]) ? b0 + 1 : b0;
+}
+
+// A grid-stride stream over the slot array, eight consecutive slots per
+// thread: the survivors per tile (atomically added into ws.status[tile],
+// which the op cleared; one atomic per warp when its 256 slots lie in one
+// tile) and, per CTA in partials s[0..2], the exact mass of the survivors,
+// their sum of |a|^4 (P2) and the exact mass of all children (when
+// truncating).  Slots rewritten by a key tie-break (kSlotKeptTie, 0) carry
+// no mass here; final_phase adds the tied children back.
+template <bool P2>
+__device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long long T, bool incl, bool trunc,
+                            i128* sRed, int* sCnt) {
+  (void)sCnt;
+  const long long n = a.in->nnz;
+  const long long nslots = (long long)ns * n;
+  const bool sums = P2 || trunc;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  const long long* part = a.ws.part;
+  i128 v[3] = {0, 0, 0};
+  const long long nchunk = (nslots + 7) >> 3;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long cb = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); cb < nchunk; cb += stride) {
+    const long long c = cb + lane;  // this thread's chunk: slots [8c, 8c + 8)
+    const long long s0 = c << 3;
+    unsigned long long x[8];
+    if (s0 + 8 <= nslots) {
+      const ulonglong2* q = reinterpret_cast<const ulonglong2*>(slots + s0);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const ulonglong2 y = q[u];
+        x[2 * u] = y.x;
+        x[2 * u + 1] = y.y;
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) x[u] = (s0 + u < nslots) ? slots[s0 + u] : ~0ULL;
+    }
+    unsigned km = 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const bool kept = slot_kept(x[u], T, incl);
+      km |= (unsigned)kept << u;
+      if (sums && x[u] != ~0ULL && x[u] != kSlotKeptTie) {
+        const i128 f = fx_from_pbits(x[u]);
+        if (trunc) v[2] += f;
+        if (kept) {
+          v[0] += f;
+          if (P2) {
+            const double p = __longlong_as_double((long long)x[u]);
+            v[1] += fx_from_pbits((unsigned long long)__double_as_longlong(__dmul_rn(p, p)));
+          }
+        }
+      }
+    }
+    // survivors per tile
+    const bool live = c < nchunk;
+    const long long last = (s0 + 7 < nslots ? s0 + 7 : nslots - 1);
+    const long long t0 = live ? tile_of(s0 / ns, kind, part) : -1;
+    const long long t1 = live ? tile_of(last / ns, kind, part) : -1;
+    const long long w0 = __shfl_sync(0xffffffffu, t0, 0);
+    const bool uniform = __all_sync(0xffffffffu, !live || (t0 == w0 && t1 == w0));
+    if (uniform) {
+      int cnt = __popc(km);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+      if (lane == 0 && cnt) atomicAdd(reinterpret_cast<unsigned long long*>(a.ws.status + w0), (unsigned long long)cnt);
+    } else if (live) {
+      for (int u = 0; u < 8; ++u) {
+        if (!((km >> u) & 1u)) continue;
+        const long long tb = (u == 0) ? t0 : tile_of((s0 + u) / ns, kind, part);
+        atomicAdd(reinterpret_cast<unsigned long long*>(a.ws.status + tb), 1ULL);
+      }
+    }
+  }
+  block_sum_i128<3>(v, sRed);
+  if (threadIdx.x == 0) {
+    Partial* pt = a.ws.partials + blockIdx.x;
+    pt->s[0] = v[0];
+    pt->s[1] = v[1];
+    pt->s[2] = v[2];
+  }
+}
+
+// Block 0 after the counts: exact kept / total mass (tied children added
+// back), the rotation decision (mode 1, the rule of bass_simulator.py:795-814:
+// the candidate's PR = kept^2 / sum |a|^4 against ctrl->pr_cur; a rejected
+// candidate is not written unless a trace is kept), and the exclusive scan of
+// the tile counts in ws.status.
+__device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j, int trace, i128* sRed) {
   SelState* sel = a.ws.sel;
-  if (threadIdx.x != 0) return;
-  const bass_state* in = a.in;
-  bass_state* out = a.out;
-  bass_ctrl* c = a.ctrl;
-  const double kept = sel->kept;
-  const long long n_in = in->nnz;
-  long long nw = sel->n_written;
-  if (nw > out->cap) {  // the write pass skipped the tiles that did not fit
-    set_error(c, BASS_ERR_CAPACITY);
-    nw = 0;
+  i128 v[3] = {0, 0, 0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    const Partial* p = a.ws.partials + b;
+    v[0] += (i128)(((u128)__ldcg((const unsigned long long*)&p->s[0] + 1) << 64) |
+                   __ldcg((const unsigned long long*)&p->s[0]));
+    v[1] += (i128)(((u128)__ldcg((const unsigned long long*)&p->s[1] + 1) << 64) |
+                   __ldcg((const unsigned long long*)&p->s[1]));
+    v[2] += (i128)(((u128)__ldcg((const unsigned long long*)&p->s[2] + 1) << 64) |
+                   __ldcg((const unsigned long long*)&p->s[2]));
   }
-  const int t = (kind == K_IDENT) ? 0 : in->pos[a.q];
-  int8_t qat[64];
-  out_order(in, kind, t, a.gb, qat);
-  for (int p = 0; p < 64; ++p) {
-    out->qat[p] = qat[p];
-    out->pos[qat[p]] = (int8_t)p;
+  block_sum_i128<3>(v, sRed);
+  if (threadIdx.x == 0) {
+    const int trunc = sel->do_trunc;
+    if (trunc && sel->tie) {  // the tied children's slots were rewritten: add them back
+      const double T = __longlong_as_double((long long)sel->t_bits);
+      const i128 f = fx_from(T);
+      v[0] += (i128)sel->need * f;
+      v[1] += (i128)sel->need * fx_from(__dmul_rn(T, T));
+      v[2] += (i128)sel->n_cand * f;
+    }
+    const double kept = fx_to(v[0]);
+    const double p2 = fx_to(v[1]);
+    sel->kept = kept;
+    sel->kept_p2 = p2;
+    if (trunc) sel->total = fx_to(v[2]);
+    if (mode == 1) {
+      const long long n_kept = trunc ? (sel->k_keep > 0 ? sel->k_keep : 0) : sel->n_out;
+      bass_ctrl* c = a.ctrl;
+      const double pr_new = (n_kept == 0 || !(p2 > 0.0)) ? INFINITY : __ddiv_rn(__dmul_rn(kept, kept), p2);
+      const bool reject = pr_new >= c->pr_cur * (1.0 - c->pr_tie_tol);
+      c->frac[j] = kept;
+      c->accept[j] = reject ? 0 : 1;
+      sel->accept = reject ? 0 : 1;
+      sel->pr_new = pr_new;
+      sel->skip_write = (reject && !trace) ? 1 : 0;
+    }
   }
-  out->nq = in->nq;
-  out->nnz = nw;
-  out->rscale[0] = 1.0;
-  out->rscale[1] = 1.0;
-  if (kind == K_PERM) return;  // first pass of a 2-qubit gate: no bookkeeping
-  c->amp_updates += n_in;
-  c->n_ops += 1;
-  const int trunc = sel->do_trunc;
-  if (mode == 1) {
-    const double nrm = sqrt(kept);
-    if (nrm > 1e-30) out->rscale[0] = 1.0 / nrm;
+  // exclusive scan of the per-tile counts
+  __shared__ long long sW[32];
+  const long long n = a.in->nnz;
+  const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const long long per = (ntiles + blockDim.x - 1) / blockDim.x;
+  const long long b0 = t * per, b1 = (b0 + per < ntiles) ? b0 + per : ntiles;
+  long long run = 0;
+  for (long long b = b0; b < b1; ++b) run += (long long)__ldcg(a.ws.status + b);
+  long long x = run;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) sW[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    long long y = (lane < (int)(blockDim.x >> 5)) ? sW[lane] : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const long long z = __shfl_up_sync(0xffffffffu, y, off);
+      if (lane >= off) y += z;
+    }
+    sW[lane] = y;
+  }
+  __syncthreads();
+  long long ex = x - run + (w > 0 ? sW[w - 1] : 0);
+  for (long long b = b0; b < b1; ++b) {
+    const long long c = (long long)__ldcg(a.ws.status + b);
+    a.ws.status[b] = (unsigned long long)ex;
+    ex += c;
+  }
+  if (t == blockDim.x - 1) {
+    sel->n_written = ex;
+    if (ex > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
+  }
+}
+
+// nblk_hist: CTAs of the evaluation pass (per-CTA child counts in partials c[0]).
+template <bool P2>
+__global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, int kind, int nblk_hist, int mode,
+                                                              int j, int trace) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned int* h = reinterpret_cast<unsigned int*>(smem);
+  __shared__ long long sS[kSelThreads];
+  __shared__ i128 sRed[3 * (kSelThreads / 32)];
+  __shared__ int sCnt[kSelThreads / 32];
+  __shared__ long long sNout;
+  __shared__ int sStage;
+  SelState* sel = a.ws.sel;
+  const int tid = threadIdx.x;
+  const long long n = a.in->nnz;
+  const long long nslots = (long long)ns * n;
+  const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
+  if (nslots > a.ws.max_n || ntiles > a.ws.max_tiles) {  // uniform: every block returns
+    if (blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
     return;
   }
-  c->last_truncated = trunc;
-  if (!trunc) return;
-  const double total = sel->total;
-  c->last_kept = kept;
-  c->last_total = total;
-  c->n_trunc += 1;
-  if (tr.gamma_mode == 1) c->gamma_running *= (total > 1e-30 ? kept / total : 0.0);
-  else if (tr.gamma_mode == 2) c->state_gamma *= (total > 1e-30 ? sqrt(kept / total) : 0.0);
-  else if (tr.gamma_mode == 3) c->state_gamma *= sqrt(kept);
-  if (tr.renorm == 1) {
-    const double nrm = sqrt(kept);
-    if (nrm > 1e-30) out->rscale[0] = 1.0 / nrm;
-  } else if (tr.renorm == 2) {
-    out->rscale[0] = 1.0 / sqrt(kept);
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  // 1. the child count
+  long long cn = 0;
+  for (int b = tid; b < nblk_hist; b += blockDim.x) cn += __ldcg(&a.ws.partials[b].c[0]);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) cn += __shfl_down_sync(0xffffffffu, cn, off);
+  if ((tid & 31) == 0) sS[tid >> 5] = cn;
+  __syncthreads();
+  if (tid == 0) {
+    long long s = 0;
+    for (int w = 0; w < kSelThreads / 32; ++w) s += sS[w];
+    sNout = s;
   }
-  if (tr.mark_active) {
-    c->truncation_active = 1;
-    c->gates_since_trunc = 0;
+  __syncthreads();
+  const long long n_out = sNout;
+  const bool trunc = !(a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out);
+  unsigned long long T = 0ULL, tkey = ~0ULL;
+  bool incl = true;
+  if (trunc && a.k_keep <= 0) {
+    T = ~0ULL;
+    tkey = 0ULL;
+    incl = false;
+  } else if (trunc) {
+    // 2. radix select on the bit patterns
+    slot_hist_phase<1>(slots, nslots, 0, h, a.ws.hist1);
+    if (!grid_sync(a)) return;
+    long long c_gt;
+    const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, sS);
+    const long long need = a.k_keep - c_gt;
+    if ((long long)__ldcg(a.ws.hist1 + b1) == need) {
+      T = (unsigned long long)b1 << 50;
+    } else {
+      slot_hist_phase<2>(slots, nslots, (unsigned long long)b1, h, a.ws.hist2);
+      if (!grid_sync(a)) return;
+      long long c_gt2;
+      const int b2 = find_bin(a.ws.hist2, need, &c_gt2, sS);
+      const long long need2 = need - c_gt2;
+      const unsigned long long pre = ((unsigned long long)b1 << 13) | (unsigned long long)b2;
+      if ((long long)__ldcg(a.ws.hist2 + b2) == need2) {
+        T = pre << 37;
+      } else {
+        scan_slots(slots, nslots, [&](unsigned long long bits, long long i) {
+          if (bits != ~0ULL && (bits >> 37) == pre) {
+            const unsigned long long k = atomicAdd(reinterpret_cast<unsigned long long*>(&sel->n_cand), 1ULL);
+            if ((long long)k < a.ws.max_n) {
+              a.ws.cand_bits[k] = bits;
+              a.ws.cand_key[k] = (unsigned long long)i;
+            } else {
+              sel->cand_overflow = 1;
+            }
+          }
+        });
+        if (blockIdx.x == 0 && tid == 0) {
+          sel->prefix = pre;
+          sel->need = need2;
+          sel->stage = 2;
+          sel->do_trunc = 1;
+          sel->n_out = n_out;
+          sel->k_keep = a.k_keep;
+        }
+        if (!grid_sync(a)) return;
+        if (blockIdx.x == 0) exact_select(a, 0, smem);
+        if (!grid_sync(a)) return;
+        if (tid == 0) sStage = *(volatile int*)&sel->stage;
+        __syncthreads();
+        if (sStage == 4) return;  // exact tie: P_GATHER and k_tie_coop continue
+        T = *(volatile unsigned long long*)&sel->t_bits;
+      }
+    }
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    sel->n_out = n_out;
+    sel->k_keep = a.k_keep;
+    sel->do_trunc = trunc ? 1 : 0;
+    sel->stage = trunc ? 3 : 0;
+    sel->t_bits = T;
+    sel->t_key = tkey;
+  }
+  // 3. survivors per tile and exact sums
+  count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, sCnt);
+  if (!grid_sync(a)) return;
+  // 4. sums, decision, tile offsets
+  if (blockIdx.x == 0) final_phase(a, gridDim.x, kind, mode, j, trace, sRed);
+}
+
+// The exact-tie continuation (only when k_select_coop stopped at stage 4 and
+// the P_GATHER pass has collected the tied children): settle the tie by key,
+// rewrite the tied slots as kept (kSlotKeptTie) or dropped (0), then steps 3-4.
+template <bool P2>
+__global__ void __launch_bounds__(kSelThreads) k_tie_coop(OpArgs a, int ns, int kind, int mode, int j,
+                                                           int trace) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ i128 sRed[3 * (kSelThreads / 32)];
+  __shared__ int sCnt[kSelThreads / 32];
+  __shared__ int sGo;
+  SelState* sel = a.ws.sel;
+  // sel->tie is set only by the selection's exact step and is not changed in
+  // this kernel, so every block takes the same branch
+  if (threadIdx.x == 0) sGo = *(volatile int*)&sel->tie;
+  __syncthreads();
+  if (!sGo) return;
+  if (blockIdx.x == 0) exact_select(a, 1, smem);
+  if (!grid_sync(a)) return;
+  const long long m0 = *(volatile long long*)&sel->n_cand;
+  const long long m = m0 < a.ws.max_n ? m0 : a.ws.max_n;
+  const long long nslots = (long long)ns * a.in->nnz;
+  const unsigned long long tk = *(volatile unsigned long long*)&sel->t_key;
+  const unsigned long long T = *(volatile unsigned long long*)&sel->t_bits;
+  unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys);
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < m;
+       k += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long i = __ldcg(a.ws.cand_bits + k);
+    if ((long long)i < nslots) slots[i] = (__ldcg(a.ws.cand_key + k) <= tk) ? kSlotKeptTie : 0ULL;
+  }
+  if (!grid_sync(a)) return;
+  count_phase<P2>(a, ns, kind, T, false, true, sRed, sCnt);
+  if (!grid_sync(a)) return;
+  if (blockIdx.x == 0) final_phase(a, gridDim.x, kind, mode, j, trace, sRed);
+}
+
+// Rotation step, after the write pass: keep the candidate if accepted.
+__global__ void k_commit(bass_state* cur, bass_state* tmp, WsView ws, bass_ctrl* c, int j, int trace) {
+  const SelState* sel = ws.sel;
+  if (!sel->accept) return;
+  bass_state t = *cur;
+  *cur = *tmp;
+  *tmp = t;
+  c->pr_cur = sel->pr_new;
+  const double frac = c->frac[j];
+  c->gamma_running *= sqrt(frac > 1e-30 ? frac : 0.0);
+  if (trace && c->trace) {
+    const long long i = c->trace_len;
+    if (i >= c->trace_cap) {
+      set_error(c, BASS_ERR_CAPACITY);
+      return;
+    }
+    uint64_t* e = c->trace + i * BASS_TRACE_WORDS;
+    e[0] = 1;
+    e[1] = (uint64_t)j;
+    for (int k = 2; k < BASS_TRACE_WORDS; ++k) e[k] = 0;
+    c->trace_len = i + 1;
   }
 }
 
@@ -1314,6 +1431,44 @@ cudaError_t zero_small(const WsView& ws, cudaStream_t s) {
   return cudaMemsetAsync(ws.counters, 0, bytes, s);
 }
 
+// Cooperative launch of the selection (tie = false) or of its exact-tie
+// continuation (tie = true); grid = every co-resident block.
+template <bool P2>
+static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace, bool tie,
+                                   cudaStream_t s) {
+  const size_t smem = (size_t)kCandSmem * 16;
+  static int grid[2] = {0, 0};
+  int& g = grid[tie ? 1 : 0];
+  if (g == 0) {
+    const void* f = tie ? (const void*)k_tie_coop<P2> : (const void*)k_select_coop<P2>;
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kSelThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    g = device().sms * occ;
+    if (g > 1024) g = 1024;  // per-CTA partials
+  }
+  a.prof = prof_on() ? 1 : 0;
+  dim3 grd(g), blk(kSelThreads);
+  cudaError_t e = cudaSuccess;
+  if (tie) {
+    void* args[] = {&a, &ns, &kind, &mode, &j, &trace};
+    KLAUNCH(S_SELECT_EXACT, s, e = cudaLaunchCooperativeKernel((const void*)k_tie_coop<P2>, grd, blk, args, smem, s));
+  } else {
+    void* args[] = {&a, &ns, &kind, &gh, &mode, &j, &trace};
+    KLAUNCH(S_SELECT1, s, e = cudaLaunchCooperativeKernel((const void*)k_select_coop<P2>, grd, blk, args, smem, s));
+  }
+  return e;
+}
+
+static cudaError_t launch_select(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace, bool tie,
+                                 cudaStream_t s) {
+  return mode == 1 ? launch_select_t<true>(a, ns, kind, gh, mode, j, trace, tie, s)
+                   : launch_select_t<false>(a, ns, kind, gh, mode, j, trace, tie, s);
+}
+
 template <int KIND>
 static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j, cudaStream_t s) {
   cudaError_t e = zero_small(a.ws, s);
@@ -1326,34 +1481,17 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
   }
   if constexpr (KIND != K_PERM) {
     constexpr int ns = slots_per_entry(KIND);
-    const int gs = device().sms * 4;
     int gh = 0;
     if ((e = launch_tile<KIND, P_HIST>(a, 0, s, &gh)) != cudaSuccess) return e;
-    KLAUNCH(S_SLOT_HIST1, s, k_slot_hist<1><<<gs, 256, 0, s>>>(a, ns, gh));
-    KLAUNCH(S_SELECT1, s, k_select1<<<1, 1024, 0, s>>>(a, gh));
-    KLAUNCH(S_SLOT_HIST2, s, k_slot_hist<2><<<gs, 256, 0, s>>>(a, ns, gh));
-    KLAUNCH(S_SELECT2, s, k_select2<<<1, 1024, 0, s>>>(a));
-    KLAUNCH(S_SLOT_GATHER, s, k_slot_gather<<<gs, 256, 0, s>>>(a, ns));
-    static bool attr = false;
-    if (!attr) {
-      e = cudaFuncSetAttribute(k_select_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, kCandSmem * 16);
-      if (e != cudaSuccess) return e;
-      attr = true;
-    }
-    KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a, 0));
+    if ((e = launch_select(a, ns, KIND, gh, fin_mode, j, tr.trace, false, s)) != cudaSuccess) return e;
     if ((e = launch_tile<KIND, P_GATHER>(a, 2, s, nullptr)) != cudaSuccess) return e;
-    KLAUNCH(S_SELECT_EXACT, s, k_select_exact<<<1, 1024, kCandSmem * 16, s>>>(a, 1));
-    KLAUNCH(S_SLOT_KEPT, s, k_tie_mark<<<device().sms, 256, 0, s>>>(a, ns));
-    if (fin_mode == 1) KLAUNCH(S_SLOT_KEPT, s, k_tile_counts<true><<<gs, 256, 0, s>>>(a, ns, KIND));
-    else KLAUNCH(S_SLOT_KEPT, s, k_tile_counts<false><<<gs, 256, 0, s>>>(a, ns, KIND));
-    KLAUNCH(S_REDUCE, s, k_kept_final<<<1, 256, 0, s>>>(a, gs, fin_mode, j, tr.trace));
-    KLAUNCH(S_REDUCE, s, k_scan_tiles<<<1, 1024, 0, s>>>(a, KIND));
+    if ((e = launch_select(a, ns, KIND, gh, fin_mode, j, tr.trace, true, s)) != cudaSuccess) return e;
   }
   a.write_mode = (KIND == K_PERM) ? 2 : 1;
-  int gw = 0;
-  if ((e = launch_tile<KIND, P_WRITE>(a, 3, s, &gw)) != cudaSuccess) return e;
-  KLAUNCH(S_FINALIZE, s, k_finalize<<<1, 32, 0, s>>>(a, tr, fin_mode, KIND));
-  return cudaGetLastError();
+  a.fin = 1;
+  a.fin_mode = fin_mode;
+  a.tr = tr;
+  return launch_tile<KIND, P_WRITE>(a, 3, s, nullptr);
 }
 
 cudaError_t run_merge_op(int kind, OpArgs a, const bass_trunc& tr, int finalize_mode, int j,
