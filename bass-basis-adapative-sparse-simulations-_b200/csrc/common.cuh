@@ -404,8 +404,9 @@ struct WsView {
   unsigned long long* cand_key;  // max_n
   SelState* sel;
   unsigned int* counters;        // 64 tile counters
-  uint64_t* tmp_keys;            // max_n
-  double2* tmp_amps;             // max_n
+  uint64_t* tmp_keys;            // max_n; gate ops: the slot array (|a|^2 bits per child)
+  double2* tmp_amps;             // max_n; gate ops: the staged children's amplitudes
+  uint64_t* stage_keys;          // max_n; gate ops: the staged children's keys
   unsigned int* sort_hist;       // radix-sort tile histograms (256 x max_tiles)
   i128* red;                     // 1024 per-CTA reduction partials
   unsigned long long* fp;        // 8 fingerprint accumulators

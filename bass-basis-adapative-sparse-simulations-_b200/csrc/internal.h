@@ -25,7 +25,7 @@ struct OpArgs {
   int drop_zero;  // K_IDENT: drop entries whose amplitude is exactly zero
   int guard;      // K_IDENT: run only if ws.sel->pad (zero flag) is set
   int prof;       // count entries into ctrl->prof_in / prof_out
-  int write_mode; // P_WRITE: 0 look-back + drop rule, 1 slot array + tile offsets, 2 one child per entry
+  int write_mode; // P_WRITE: 0 look-back + drop rule, 2 one child per entry
   int fin;        // P_WRITE: the last CTA to finish writes the output descriptor (finalize_op)
   int fin_mode;   // finalize_op: 0 gate / truncation, 1 rotation step
   long long k_cond, k_keep;

@@ -552,37 +552,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
         pt->s[0] = v[0]; pt->s[1] = v[1]; pt->s[2] = v[2]; pt->s[3] = v[3];
       }
     } else if (PASS == P_WRITE) {
-      // write_mode 1: kept children from the slot array, tile base from
-      //   the selection's tile scan; 2: one child per entry, base = the tile's Z start;
-      //   0: the drop rule decides, base by decoupled look-back.
+      // write_mode 2: one child per entry (a 2-qubit gate's first pass),
+      //   base = the tile's Z start; 0: the drop rule decides (diagonal
+      //   1-qubit gate compaction), base by decoupled look-back.  Gates,
+      //   rotations and truncations write through k_compact instead.
       constexpr int MC = KindTraits<KIND>::kMaxChildren;
       uint64_t kb;
       double2 ca[MC];
       uint16_t* sOff = sIdx;                              // free after the merge
       uint8_t* sMask = reinterpret_cast<uint8_t*>(sK);    // free after the merge
       const int wmode = a.write_mode;
-      const unsigned long long T = S.do_trunc ? S.t_bits : 0ULL;
-      const bool incl = !S.do_trunc || S.t_key == ~0ULL;
-      const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys) + NS * sZstart;
       // (a) kept-children mask per position
       for (int p = tid; p < E; p += kThreads) {
         unsigned mk = 0;
-        if (wmode == 1) {
-          unsigned long long sb[NS];
-          if (NS == 1) {
-            sb[0] = slots[p];
-          } else {
-#pragma unroll
-            for (int c = 0; c < NS; c += 2) {
-              const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(slots + (long long)NS * p + c);
-              sb[c] = v.x;
-              sb[c + 1] = v.y;
-            }
-          }
-#pragma unroll
-          for (int c = 0; c < NS; ++c)
-            if (slot_kept(sb[c], T, incl)) mk |= 1u << c;
-        } else if (wmode == 2) {
+        if (wmode == 2) {
           mk = 1u;
         } else {
           const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
@@ -615,7 +598,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
           if (tid == 0) sBase = b;
         }
       } else if (tid == 0) {
-        sBase = (wmode == 1) ? (long long)a.ws.status[tile] : sZstart;
+        sBase = sZstart;
       }
       __syncthreads();
       if (tid == 0) {
@@ -645,9 +628,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
         }
       }
     } else if (PASS == P_HIST) {
+      // every child is staged at its slot index: |a|^2 bits in the slot
+      // array, key and amplitude in the staging arrays (the write step
+      // compacts the survivors from there)
       uint64_t kb;
       double2 ca[NS];
       unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys) + NS * sZstart;
+      uint64_t* skeys = a.ws.stage_keys + NS * sZstart;
+      double2* samps = a.ws.tmp_amps + NS * sZstart;
       for (int p = tid; p < E; p += kThreads) {
         const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
         unsigned long long sb[NS];
@@ -658,6 +646,19 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
             ++cnt;
           } else {
             sb[c] = ~0ULL;
+          }
+        }
+        if (cm) {  // every slot of the group is written (a missing child's slot holds ~0 bits)
+          if (NS == 1) {
+            skeys[p] = kb;
+            samps[p] = ca[0];
+          } else {
+#pragma unroll
+            for (int c = 0; c < NS; c += 2)
+              *reinterpret_cast<ulonglong2*>(skeys + (long long)NS * p + c) =
+                  make_ulonglong2(kb | (uint64_t)c, kb | (uint64_t)(c + 1));
+#pragma unroll
+            for (int c = 0; c < NS; ++c) samps[(long long)NS * p + c] = ca[c];
           }
         }
         if (NS == 1) {
@@ -1358,6 +1359,113 @@ __global__ void __launch_bounds__(kSelThreads) k_tie_coop(OpArgs a, int ns, int 
   if (blockIdx.x == 0) final_phase(a, gridDim.x, kind, mode, j, trace, sRed);
 }
 
+// ---------------------------------------------------------------------------
+// the write step of a gate / rotation / truncation: compaction
+// ---------------------------------------------------------------------------
+// One CTA per tile (block-strided).  The tile's children sit at its slot
+// range [NS * P'_b, NS * P'_{b+1}) of the staging arrays, in output order; the
+// survivors (decided by the slot alone, see slot_kept) are written from the
+// tile's base (the selection's scan of the tile counts) on, eight consecutive
+// slots per thread and round.  The last CTA to finish writes the output
+// descriptor.  A rejected rotation candidate is not written.
+__global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
+  __shared__ SelState S;
+  __shared__ int sCnt[8][kThreads / 32];  // survivors per (round u, warp)
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid == 0) S = *a.ws.sel;
+  __syncthreads();
+  const long long n = a.in->nnz;
+  const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
+  const bool ok = ntiles <= a.ws.max_tiles && (long long)ns * n <= a.ws.max_n;
+  if (!ok && blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+  const unsigned long long T = S.do_trunc ? S.t_bits : 0ULL;
+  const bool incl = !S.do_trunc || S.t_key == ~0ULL;
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  uint64_t* okeys = a.out->keys;
+  double2* oamps = reinterpret_cast<double2*>(a.out->amps);
+  const long long cap = a.out->cap;
+  const unsigned lt = (1u << lane) - 1;
+  long long written = 0;
+  for (long long b = blockIdx.x; ok && !S.skip_write && b < ntiles; b += gridDim.x) {
+    long long z0, z1;
+    if (kind == K_IDENT) {
+      z0 = b * kTile;
+      z1 = (z0 + kTile < n) ? z0 + kTile : n;
+    } else {
+      z0 = a.ws.part[b * 6];
+      z1 = a.ws.part[(b + 1) * 6];
+    }
+    const long long s1 = ns * z1;
+    long long base = (long long)a.ws.status[b];
+    // rounds of 8 x 256 slots; slot (u, tid) = i0 + 256 u + tid, so every
+    // warp load and store covers consecutive slots
+    for (long long i0 = ns * z0; i0 < s1; i0 += 8 * kThreads) {
+      // all loads of the round first, then the ranks, then the stores
+      unsigned long long x[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const long long i = i0 + u * kThreads + tid;
+        x[u] = (i < s1) ? __ldcs(slots + i) : ~0ULL;
+      }
+      unsigned bal[8];
+      unsigned long long kk[8];
+      double2 aa[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const long long i = i0 + u * kThreads + tid;
+        const bool kept = slot_kept(x[u], T, incl);
+        bal[u] = __ballot_sync(0xffffffffu, kept);
+        if (kept) {
+          kk[u] = __ldcs(a.ws.stage_keys + i);
+          aa[u] = __ldcs(a.ws.tmp_amps + i);
+        }
+        if (lane == 0) sCnt[u][w] = __popc(bal[u]);
+      }
+      __syncthreads();
+      int tot = 0;  // survivors of the round
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int v = 0; v < kThreads / 32; ++v) tot += sCnt[u][v];
+      if (base + tot <= cap) {
+        int run = 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          int ahead = run;
+#pragma unroll
+          for (int v = 0; v < kThreads / 32; ++v)
+            if (v < w) ahead += sCnt[u][v];
+          if ((bal[u] >> lane) & 1u) {
+            const long long o = base + ahead + __popc(bal[u] & lt);
+            okeys[o] = kk[u];
+            oamps[o] = aa[u];
+          }
+#pragma unroll
+          for (int v = 0; v < kThreads / 32; ++v) run += sCnt[u][v];
+        }
+      } else if (tid == 0) {
+        set_error(a.ctrl, BASS_ERR_CAPACITY);
+      }
+      base += tot;
+      written += tot;
+      __syncthreads();  // sCnt is reused by the next round
+    }
+  }
+  if (tid == 0 && a.prof && written)
+    atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_out[kind * 5 + P_WRITE]),
+              (unsigned long long)written);
+  // the last CTA to finish writes the output descriptor
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    const unsigned long long d = atomicAdd(&reinterpret_cast<unsigned long long*>(a.ws.counters)[59], 1ULL);
+    if (d == gridDim.x - 1) {
+      __threadfence();
+      finalize_op(a, a.tr, a.fin_mode, kind);
+    }
+  }
+}
+
 // Rotation step, after the write pass: keep the candidate if accepted.
 __global__ void k_commit(bass_state* cur, bass_state* tmp, WsView ws, bass_ctrl* c, int j, int trace) {
   const SelState* sel = ws.sel;
@@ -1487,11 +1595,18 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
     if ((e = launch_tile<KIND, P_GATHER>(a, 2, s, nullptr)) != cudaSuccess) return e;
     if ((e = launch_select(a, ns, KIND, gh, fin_mode, j, tr.trace, true, s)) != cudaSuccess) return e;
   }
-  a.write_mode = (KIND == K_PERM) ? 2 : 1;
   a.fin = 1;
   a.fin_mode = fin_mode;
   a.tr = tr;
-  return launch_tile<KIND, P_WRITE>(a, 3, s, nullptr);
+  if constexpr (KIND == K_PERM) {
+    a.write_mode = 2;
+    return launch_tile<KIND, P_WRITE>(a, 3, s, nullptr);
+  } else {
+    a.prof = prof_on() ? 1 : 0;
+    KLAUNCH(KIND * 5 + P_WRITE, s,
+            k_compact<<<device().sms * 4, kThreads, 0, s>>>(a, slots_per_entry(KIND), KIND));
+    return cudaGetLastError();
+  }
 }
 
 cudaError_t run_merge_op(int kind, OpArgs a, const bass_trunc& tr, int finalize_mode, int j,
