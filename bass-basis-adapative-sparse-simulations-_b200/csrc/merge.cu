@@ -737,8 +737,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
 //      finds the boundary bins itself, so each level costs one grid barrier;
 //   3. per tile, the number of survivors (into ws.status) and per CTA the
 //      exact kept mass, total mass and, for a rotation step, sum of |a|^4;
-//   4. block 0: the exact sums, the rotation decision, and an exclusive scan
-//      of the tile counts (each tile of the write pass then knows its base).
+//   4. the last block to finish step 3: the exact sums, the rotation
+//      decision, and an exclusive scan of the tile counts (each tile of the
+//      write step then knows its base).
 // An exact tie at the threshold (equal bit patterns straddling rank k) stops
 // it after step 2; the tied children's keys are then collected by the tile
 // kernel's P_GATHER pass and k_tie_coop settles the tie by key and runs
@@ -780,16 +781,19 @@ __device__ bool grid_sync(const OpArgs& a) {
 }
 
 // Block-wide: the bin b of an 8192-bin histogram (in global memory, written by
-// other blocks) with count(bins > b) < k <= count(bins >= b); *c_gt =
-// count(bins > b).  Needs 1 <= k <= total and blockDim.x dividing 8192.
-__device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, long long* sS) {
+// other blocks; copied to hs, kHistBins words of shared memory) with
+// count(bins > b) < k <= count(bins >= b); *c_gt = count(bins > b).  Needs
+// 1 <= k <= total and blockDim.x dividing 8192.
+__device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, long long* sS, unsigned int* hs) {
   __shared__ int sRes;
   __shared__ long long sAbove;
   const int t = threadIdx.x, nt = blockDim.x;
   const int per = kHistBins / nt;   // bins per thread
   const int lanes_per = nt / 32;    // sS entries per lane of warp 0
+  for (int i = t; i < kHistBins; i += nt) hs[i] = __ldcg(hist + i);
+  __syncthreads();
   long long s = 0;
-  for (int i = 0; i < per; ++i) s += __ldcg(hist + per * t + i);
+  for (int i = 0; i < per; ++i) s += hs[per * t + i];
   sS[t] = s;
   __syncthreads();
   if (t < 32) {
@@ -812,7 +816,7 @@ __device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, 
       }
       int b = per * tt + per - 1;
       for (; b > per * tt; --b) {
-        const long long h = __ldcg(hist + b);
+        const long long h = hs[b];
         if (above + h >= k) break;
         above += h;
       }
@@ -939,21 +943,27 @@ __device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem) {
   __shared__ long long sGt, sEq;
   if (m <= kCandSmem) {
     sort_candidates(sb, sk, m, a.ws, mode == 1);
-    if (tid == 0) {
-      const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
-      if (mode == 1) {
+    const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
+    if (mode == 1) {
+      if (tid == 0) {
         sel->t_bits = sPre;
         sel->t_key = sk[r];
         sel->stage = 3;
-      } else {
-        const unsigned long long T = sb[r];
-        long long gt = 0, eq = 0;
-        for (long long i = 0; i < m; ++i) {
-          gt += sb[i] > T;
-          eq += sb[i] == T;
-        }
-        sT = T; sGt = gt; sEq = eq;
       }
+    } else {
+      // sorted descending: the entries above T precede the run equal to T
+      const unsigned long long T = sb[r];
+      __shared__ int sLo, sHi;
+      if (tid == 0) { sLo = (int)r; sHi = (int)r; }
+      __syncthreads();
+      for (long long i = tid; i < m; i += blockDim.x) {
+        if (sb[i] == T) {
+          atomicMin(&sLo, (int)i);
+          atomicMax(&sHi, (int)i);
+        }
+      }
+      __syncthreads();
+      if (tid == 0) { sT = T; sGt = sLo; sEq = sHi - sLo + 1; }
     }
   } else if (mode == 1) {
     // all candidates share the bit pattern: radix select of the need-th smallest key
@@ -1068,6 +1078,7 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
   const long long n = a.in->nnz;
   const long long nslots = (long long)ns * n;
   const bool sums = P2 || trunc;
+  const bool want_total = trunc && !P2;  // gamma bookkeeping of plain truncations only
   const int lane = threadIdx.x & 31;
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
   const long long* part = a.ws.part;
@@ -1097,7 +1108,7 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
       km |= (unsigned)kept << u;
       if (sums && x[u] != ~0ULL && x[u] != kSlotKeptTie) {
         const i128 f = fx_from_pbits(x[u]);
-        if (trunc) v[2] += f;
+        if (want_total) v[2] += f;
         if (kept) {
           v[0] += f;
           if (P2) {
@@ -1136,13 +1147,13 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
   }
 }
 
-// Block 0 after the counts: exact kept / total mass (tied children added
+// The last block after the counts: exact kept / total mass (tied children added
 // back), the rotation decision (mode 1, the rule of bass_simulator.py:795-814:
 // the candidate's PR = kept^2 / sum |a|^4 against ctrl->pr_cur; a rejected
 // candidate is not written unless a trace is kept), and the exclusive scan of
 // the tile counts in ws.status.
 __device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j, int trace, i128* sRed) {
-  SelState* sel = a.ws.sel;
+  volatile SelState* sel = a.ws.sel;  // written by other blocks of this kernel
   i128 v[3] = {0, 0, 0};
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
     const Partial* p = a.ws.partials + b;
@@ -1180,43 +1191,61 @@ __device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j
       sel->skip_write = (reject && !trace) ? 1 : 0;
     }
   }
-  // exclusive scan of the per-tile counts
+  // exclusive scan of the per-tile counts, in coalesced rounds of blockDim
   __shared__ long long sW[32];
+  __shared__ long long sCarry;
   const long long n = a.in->nnz;
   const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const long long per = (ntiles + blockDim.x - 1) / blockDim.x;
-  const long long b0 = t * per, b1 = (b0 + per < ntiles) ? b0 + per : ntiles;
-  long long run = 0;
-  for (long long b = b0; b < b1; ++b) run += (long long)__ldcg(a.ws.status + b);
-  long long x = run;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const long long y = __shfl_up_sync(0xffffffffu, x, off);
-    if (lane >= off) x += y;
-  }
-  if (lane == 31) sW[w] = x;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
+  if (t == 0) sCarry = 0;
   __syncthreads();
-  if (w == 0) {
-    long long y = (lane < (int)(blockDim.x >> 5)) ? sW[lane] : 0;
+  for (long long r0 = 0; r0 < ntiles; r0 += blockDim.x) {
+    const long long b = r0 + t;
+    const long long c = (b < ntiles) ? (long long)__ldcg(a.ws.status + b) : 0;
+    long long x = c;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const long long z = __shfl_up_sync(0xffffffffu, y, off);
-      if (lane >= off) y += z;
+      const long long y = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= off) x += y;
     }
-    sW[lane] = y;
+    if (lane == 31) sW[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      long long y = (lane < nw) ? sW[lane] : 0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const long long z = __shfl_up_sync(0xffffffffu, y, off);
+        if (lane >= off) y += z;
+      }
+      if (lane < nw) sW[lane] = y;
+    }
+    __syncthreads();
+    const long long carry = sCarry;
+    const long long incl = x + (w > 0 ? sW[w - 1] : 0);
+    if (b < ntiles) a.ws.status[b] = (unsigned long long)(carry + incl - c);
+    __syncthreads();
+    if (t == blockDim.x - 1) sCarry = carry + incl;
+    __syncthreads();
+  }
+  if (t == 0) {
+    sel->n_written = sCarry;
+    if (sCarry > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
+  }
+}
+
+// After count_phase: the last block to finish runs final_phase (the others
+// exit), which needs every block's partial sums and tile counts.
+__device__ void finish_by_last_block(const OpArgs& a, int kind, int mode, int j, int trace, i128* sRed) {
+  __shared__ int sLast;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned long long d = atomicAdd(&reinterpret_cast<unsigned long long*>(a.ws.counters)[58], 1ULL);
+    sLast = (d == gridDim.x - 1);
+    __threadfence();
   }
   __syncthreads();
-  long long ex = x - run + (w > 0 ? sW[w - 1] : 0);
-  for (long long b = b0; b < b1; ++b) {
-    const long long c = (long long)__ldcg(a.ws.status + b);
-    a.ws.status[b] = (unsigned long long)ex;
-    ex += c;
-  }
-  if (t == blockDim.x - 1) {
-    sel->n_written = ex;
-    if (ex > a.out->cap) set_error(a.ctrl, BASS_ERR_CAPACITY);
-  }
+  if (sLast) final_phase(a, gridDim.x, kind, mode, j, trace, sRed);
 }
 
 // nblk_hist: CTAs of the evaluation pass (per-CTA child counts in partials c[0]).
@@ -1266,18 +1295,18 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
     slot_hist_phase<1>(slots, nslots, 0, h, a.ws.hist1);
     if (!grid_sync(a)) return;
     long long c_gt;
-    const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, sS);
+    const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, sS, h);
     const long long need = a.k_keep - c_gt;
-    if ((long long)__ldcg(a.ws.hist1 + b1) == need) {
+    if ((long long)h[b1] == need) {
       T = (unsigned long long)b1 << 50;
     } else {
       slot_hist_phase<2>(slots, nslots, (unsigned long long)b1, h, a.ws.hist2);
       if (!grid_sync(a)) return;
       long long c_gt2;
-      const int b2 = find_bin(a.ws.hist2, need, &c_gt2, sS);
+      const int b2 = find_bin(a.ws.hist2, need, &c_gt2, sS, h);
       const long long need2 = need - c_gt2;
       const unsigned long long pre = ((unsigned long long)b1 << 13) | (unsigned long long)b2;
-      if ((long long)__ldcg(a.ws.hist2 + b2) == need2) {
+      if ((long long)h[b2] == need2) {
         T = pre << 37;
       } else {
         scan_slots(slots, nslots, [&](unsigned long long bits, long long i) {
@@ -1319,9 +1348,8 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
   }
   // 3. survivors per tile and exact sums
   count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, sCnt);
-  if (!grid_sync(a)) return;
   // 4. sums, decision, tile offsets
-  if (blockIdx.x == 0) final_phase(a, gridDim.x, kind, mode, j, trace, sRed);
+  finish_by_last_block(a, kind, mode, j, trace, sRed);
 }
 
 // The exact-tie continuation (only when k_select_coop stopped at stage 4 and
@@ -1355,8 +1383,7 @@ __global__ void __launch_bounds__(kSelThreads) k_tie_coop(OpArgs a, int ns, int 
   }
   if (!grid_sync(a)) return;
   count_phase<P2>(a, ns, kind, T, false, true, sRed, sCnt);
-  if (!grid_sync(a)) return;
-  if (blockIdx.x == 0) final_phase(a, gridDim.x, kind, mode, j, trace, sRed);
+  finish_by_last_block(a, kind, mode, j, trace, sRed);
 }
 
 // ---------------------------------------------------------------------------
