@@ -88,8 +88,8 @@ static Layout layout_for(long long max_n) {
   L.sort_tiles = max_n / 2048 + 2;
   size_t o = 0;
   L.counters = o; o += align256(64 * 8);
-  L.hist1 = o; o += align256(kHistBins * 4);
-  L.hist2 = o; o += align256(kHistBins * 4);
+  L.hist1 = o; o += align256((kHistBins + kHistGroups) * 4);
+  L.hist2 = o; o += align256((kHistBins + kHistGroups) * 4);
   L.sel = o; o += align256(sizeof(SelState));
   L.status = o; o += align256((size_t)L.max_tiles * 8);
   L.fp = o; o += align256(8 * 8);

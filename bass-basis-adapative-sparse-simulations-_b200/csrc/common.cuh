@@ -28,6 +28,8 @@ constexpr int kPerThread = kTile / kThreads;
 constexpr int kStep = kTile - 8;
 constexpr int kTilePad = kTile + 8;
 constexpr int kHistBins = 8192;      // 13-bit radix-select digits
+constexpr int kGroupBins = 128;      // bins per coarse group of a selection histogram
+constexpr int kHistGroups = kHistBins / kGroupBins;  // coarse counts stored after the bins
 constexpr int kCandSmem = 4096;      // candidates sorted in shared memory
 constexpr int kMaxSets = 64;         // partition sets (one per qubit for RDMs)
 constexpr int kFxFrac = 96;
@@ -391,14 +393,15 @@ struct SelState {
   int accept;            // rotation step: the candidate lowers PR
   double pr_new;         // rotation step: PR of the candidate
   int tie;               // the threshold was settled by key (stage 4 was taken)
-  int pad3;
+  int tie_overflow;      // the tied children did not fit the candidate arrays
+  long long n_tie;       // tied children collected by the P_GATHER pass
 };
 
 struct WsView {
   long long* part;               // kMaxSets x (max_tiles + 1) x 6
   unsigned long long* status;    // max_tiles
-  unsigned int* hist1;           // kHistBins
-  unsigned int* hist2;           // kHistBins
+  unsigned int* hist1;           // kHistBins bins, then kHistGroups coarse counts
+  unsigned int* hist2;           // kHistBins bins, then kHistGroups coarse counts
   Partial* partials;             // kMaxSets x max_tiles
   unsigned long long* cand_bits; // max_n
   unsigned long long* cand_key;  // max_n

@@ -681,12 +681,12 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
           const uint64_t bits = (uint64_t)__double_as_longlong(prob(ca[c]));
           if (bits == S.prefix) {
             const unsigned long long slot =
-                atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws.sel->n_cand), 1ULL);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws.sel->n_tie), 1ULL);
             if ((long long)slot < a.ws.max_n) {
               a.ws.cand_bits[slot] = (unsigned long long)(NS * (sZstart + p) + c);  // its slot index
               a.ws.cand_key[slot] = true_key(kb | (uint64_t)c, H.qat_out, 64);
             } else {
-              a.ws.sel->cand_overflow = 1;
+              a.ws.sel->tie_overflow = 1;
             }
           }
         }
@@ -780,52 +780,64 @@ __device__ bool grid_sync(const OpArgs& a) {
   return sOk != 0;
 }
 
-// Block-wide: the bin b of an 8192-bin histogram (in global memory, written by
-// other blocks; copied to hs, kHistBins words of shared memory) with
-// count(bins > b) < k <= count(bins >= b); *c_gt = count(bins > b).  Needs
-// 1 <= k <= total and blockDim.x dividing 8192.
-__device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, long long* sS, unsigned int* hs) {
+// Block-wide (warp 0 works): the bin b of an 8192-bin histogram in global
+// memory (written by other blocks, with coarse counts of its 64 groups of 128
+// bins after the bins) with count(bins > b) < k <= count(bins >= b);
+// *c_gt = count(bins > b), *c_b = count(b).  Needs 1 <= k <= total.  Reads the
+// 64 coarse counts and the 128 bins of one group.
+__device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, long long* c_b) {
   __shared__ int sRes;
-  __shared__ long long sAbove;
-  const int t = threadIdx.x, nt = blockDim.x;
-  const int per = kHistBins / nt;   // bins per thread
-  const int lanes_per = nt / 32;    // sS entries per lane of warp 0
-  for (int i = t; i < kHistBins; i += nt) hs[i] = __ldcg(hist + i);
-  __syncthreads();
-  long long s = 0;
-  for (int i = 0; i < per; ++i) s += hs[per * t + i];
-  sS[t] = s;
-  __syncthreads();
-  if (t < 32) {
-    long long ls = 0;
-    for (int i = 0; i < lanes_per; ++i) ls += sS[lanes_per * t + i];
-    long long suf = ls;
+  __shared__ long long sAbove, sCnt;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    // coarse: lane holds groups 2 lane and 2 lane + 1
+    const long long g0 = __ldcg(hist + kHistBins + 2 * lane);
+    const long long g1 = __ldcg(hist + kHistBins + 2 * lane + 1);
+    const long long v = g0 + g1;
+    long long suf = v;  // groups >= 2 lane
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const long long v = __shfl_down_sync(0xffffffffu, suf, off);
-      if (t + off < 32) suf += v;
+      const long long y = __shfl_down_sync(0xffffffffu, suf, off);
+      if (lane + off < 32) suf += y;
     }
     const unsigned m = __ballot_sync(0xffffffffu, suf >= k);
     const int L = m ? 31 - __clz(m) : 0;
-    if (t == L) {
-      long long above = suf - ls;
-      int tt = lanes_per * L + lanes_per - 1;
-      for (; tt > lanes_per * L; --tt) {
-        if (above + sS[tt] >= k) break;
-        above += sS[tt];
+    long long above = __shfl_sync(0xffffffffu, suf - v, L);  // groups > 2 L + 1
+    const long long c1 = __shfl_sync(0xffffffffu, g1, L);
+    int G = 2 * L + 1;
+    if (above + c1 < k) {
+      above += c1;
+      G = 2 * L;
+    }
+    // fine: lane holds bins 128 G + 4 lane .. + 3
+    const unsigned* hb = hist + G * kGroupBins + 4 * lane;
+    long long f[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) f[q] = __ldcg(hb + q);
+    const long long w = f[0] + f[1] + f[2] + f[3];
+    long long suf2 = w;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const long long y = __shfl_down_sync(0xffffffffu, suf2, off);
+      if (lane + off < 32) suf2 += y;
+    }
+    const unsigned m2 = __ballot_sync(0xffffffffu, above + suf2 >= k);
+    const int L2 = m2 ? 31 - __clz(m2) : 0;
+    if (lane == L2) {
+      long long ab = above + suf2 - w;  // bins above this lane's four
+      int q = 3;
+      for (; q > 0; --q) {
+        if (ab + f[q] >= k) break;
+        ab += f[q];
       }
-      int b = per * tt + per - 1;
-      for (; b > per * tt; --b) {
-        const long long h = hs[b];
-        if (above + h >= k) break;
-        above += h;
-      }
-      sRes = b;
-      sAbove = above;
+      sRes = G * kGroupBins + 4 * lane + q;
+      sAbove = ab;
+      sCnt = f[q];
     }
   }
   __syncthreads();
   *c_gt = sAbove;
+  *c_b = sCnt;
   return sRes;
 }
 
@@ -869,6 +881,17 @@ __device__ void slot_hist_phase(const unsigned long long* slots, long long nslot
   __syncthreads();
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
     if (h[i]) atomicAdd(&gh[i], h[i]);
+  // coarse counts of 64 groups of 128 bins (gh[kHistBins + g]), for find_bin
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int g = w; g < kHistGroups; g += nw) {
+    const unsigned* hg = h + g * kGroupBins;
+    unsigned c = 0;
+#pragma unroll
+    for (int q = 0; q < kGroupBins / 32; ++q) c += hg[32 * q + lane];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+    if (lane == 0 && c) atomicAdd(&gh[kHistBins + g], c);
+  }
 }
 
 // better(a, b): a ranks strictly above b
@@ -913,28 +936,40 @@ __device__ void sort_candidates(unsigned long long* sb, unsigned long long* sk, 
   }
 }
 
-// One block.  mode 0 (stage 2): candidates are (bits, slot) of the level-2
-//   boundary bin; find the need-th largest bit pattern T.  If every candidate
-//   equal to T is needed the threshold is resolved (keep bits >= T, stage 3);
+// Result of exact_select (in shared memory of the calling block).
+struct ExactOut {
+  int stage;                 // 3 resolved, 4 exact tie to settle by key
+  unsigned long long t_bits; // stage 3: the threshold bit pattern
+  unsigned long long t_key;  // stage 3: ~0 (every child at t_bits kept) or the largest kept key
+  unsigned long long prefix; // stage 4: the tied bit pattern
+  long long need;            // stage 4: tied children to keep
+};
+
+// One block.  mode 0: the m candidates (bits, slot) of the level-2 boundary
+//   bin (pre, need: its 26-bit prefix and the survivors still to take from
+//   it); find the need-th largest bit pattern T.  If every candidate equal to
+//   T is needed the threshold is resolved (keep bits >= T, stage 3);
 //   otherwise the tie is settled by true key (stage 4: the tied children are
-//   collected with their keys).
-// mode 1 (stage 4): candidates are (slot, true key) of the children at T;
-//   keep the need smallest keys (stage 3 with t_key).
-__device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem) {
+//   collected with their keys).  Several blocks may run it on the same
+//   candidates; only the one with writer set writes the selection state.
+// mode 1 (stage 4, one block): the candidates are (slot, true key) of the
+//   children at T; keep the need smallest keys (stage 3 with t_key).
+__device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem, long long m_in, bool overflow,
+                             long long need_in, unsigned long long pre_in, bool writer, ExactOut* out) {
   unsigned long long* sb = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* sk = sb + kCandSmem;
   SelState* sel = a.ws.sel;
   __shared__ long long sM, sNeedIn;
   __shared__ unsigned long long sPre;
   if (threadIdx.x == 0) {
-    long long m = *(volatile long long*)&sel->n_cand;
-    if (*(volatile int*)&sel->cand_overflow || m > a.ws.max_n) {
-      set_error(a.ctrl, BASS_ERR_WORKSPACE);
+    long long m = m_in;
+    if (overflow || m > a.ws.max_n) {
+      if (writer) set_error(a.ctrl, BASS_ERR_WORKSPACE);
       m = a.ws.max_n;
     }
     sM = m;
-    sNeedIn = sel->need;
-    sPre = sel->prefix;
+    sNeedIn = need_in;
+    sPre = pre_in;
   }
   __syncthreads();
   const long long m = sM, need = sNeedIn;
@@ -946,9 +981,14 @@ __device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem) {
     const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
     if (mode == 1) {
       if (tid == 0) {
-        sel->t_bits = sPre;
-        sel->t_key = sk[r];
-        sel->stage = 3;
+        out->stage = 3;
+        out->t_bits = sPre;
+        out->t_key = sk[r];
+        if (writer) {
+          sel->t_bits = sPre;
+          sel->t_key = sk[r];
+          sel->stage = 3;
+        }
       }
     } else {
       // sorted descending: the entries above T precede the run equal to T
@@ -994,9 +1034,14 @@ __device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem) {
       __syncthreads();
     }
     if (tid == 0) {
-      sel->t_bits = sPre;
-      sel->t_key = sKeyPre;
-      sel->stage = 3;
+      out->stage = 3;
+      out->t_bits = sPre;
+      out->t_key = sKeyPre;
+      if (writer) {
+        sel->t_bits = sPre;
+        sel->t_key = sKeyPre;
+        sel->stage = 3;
+      }
     }
     __syncthreads();
     return;
@@ -1041,16 +1086,24 @@ __device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem) {
   if (tid == 0 && mode == 0) {
     const long long take = need - sGt;  // entries equal to T that are kept
     if (take == sEq) {
-      sel->t_bits = sT;
-      sel->t_key = ~0ULL;
-      sel->stage = 3;
+      out->stage = 3;
+      out->t_bits = sT;
+      out->t_key = ~0ULL;
+      if (writer) {
+        sel->t_bits = sT;
+        sel->t_key = ~0ULL;
+        sel->stage = 3;
+      }
     } else {
-      sel->stage = 4;
-      sel->tie = 1;
-      sel->prefix = sT;
-      sel->need = take;
-      sel->n_cand = 0;
-      sel->cand_overflow = 0;
+      out->stage = 4;
+      out->prefix = sT;
+      out->need = take;
+      if (writer) {
+        sel->stage = 4;
+        sel->tie = 1;
+        sel->prefix = sT;
+        sel->need = take;
+      }
     }
   }
   __syncthreads();
@@ -1172,7 +1225,7 @@ __device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j
       const i128 f = fx_from(T);
       v[0] += (i128)sel->need * f;
       v[1] += (i128)sel->need * fx_from(__dmul_rn(T, T));
-      v[2] += (i128)sel->n_cand * f;
+      v[2] += (i128)sel->n_tie * f;
     }
     const double kept = fx_to(v[0]);
     const double p2 = fx_to(v[1]);
@@ -1254,11 +1307,10 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
                                                               int j, int trace) {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned int* h = reinterpret_cast<unsigned int*>(smem);
-  __shared__ long long sS[kSelThreads];
+  __shared__ long long sS[kSelThreads / 32];
   __shared__ i128 sRed[3 * (kSelThreads / 32)];
   __shared__ int sCnt[kSelThreads / 32];
   __shared__ long long sNout;
-  __shared__ int sStage;
   SelState* sel = a.ws.sel;
   const int tid = threadIdx.x;
   const long long n = a.in->nnz;
@@ -1294,19 +1346,19 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
     // 2. radix select on the bit patterns
     slot_hist_phase<1>(slots, nslots, 0, h, a.ws.hist1);
     if (!grid_sync(a)) return;
-    long long c_gt;
-    const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, sS, h);
+    long long c_gt, c_b1;
+    const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, &c_b1);
     const long long need = a.k_keep - c_gt;
-    if ((long long)h[b1] == need) {
+    if (c_b1 == need) {
       T = (unsigned long long)b1 << 50;
     } else {
       slot_hist_phase<2>(slots, nslots, (unsigned long long)b1, h, a.ws.hist2);
       if (!grid_sync(a)) return;
-      long long c_gt2;
-      const int b2 = find_bin(a.ws.hist2, need, &c_gt2, sS, h);
+      long long c_gt2, c_b2;
+      const int b2 = find_bin(a.ws.hist2, need, &c_gt2, &c_b2);
       const long long need2 = need - c_gt2;
       const unsigned long long pre = ((unsigned long long)b1 << 13) | (unsigned long long)b2;
-      if ((long long)h[b2] == need2) {
+      if (c_b2 == need2) {
         T = pre << 37;
       } else {
         scan_slots(slots, nslots, [&](unsigned long long bits, long long i) {
@@ -1329,12 +1381,30 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
           sel->k_keep = a.k_keep;
         }
         if (!grid_sync(a)) return;
-        if (blockIdx.x == 0) exact_select(a, 0, smem);
-        if (!grid_sync(a)) return;
-        if (tid == 0) sStage = *(volatile int*)&sel->stage;
+        // few candidates (the usual case): every block settles them itself,
+        // block 0 records the result; many: block 0 alone, then a barrier
+        __shared__ ExactOut eo;
+        __shared__ long long sMc;
+        __shared__ int sOvf;
+        if (tid == 0) {
+          sMc = *(volatile long long*)&sel->n_cand;
+          sOvf = *(volatile int*)&sel->cand_overflow;
+        }
         __syncthreads();
-        if (sStage == 4) return;  // exact tie: P_GATHER and k_tie_coop continue
-        T = *(volatile unsigned long long*)&sel->t_bits;
+        const long long mc = sMc;
+        if (mc <= kCandSmem && !sOvf) {
+          exact_select(a, 0, smem, mc, false, need2, pre, blockIdx.x == 0, &eo);
+        } else {
+          if (blockIdx.x == 0) exact_select(a, 0, smem, mc, sOvf != 0, need2, pre, true, &eo);
+          if (!grid_sync(a)) return;
+          if (tid == 0) {
+            eo.stage = *(volatile int*)&sel->stage;
+            eo.t_bits = *(volatile unsigned long long*)&sel->t_bits;
+          }
+          __syncthreads();
+        }
+        if (eo.stage == 4) return;  // exact tie: P_GATHER and k_tie_coop continue
+        T = eo.t_bits;
       }
     }
   }
@@ -1368,9 +1438,13 @@ __global__ void __launch_bounds__(kSelThreads) k_tie_coop(OpArgs a, int ns, int 
   if (threadIdx.x == 0) sGo = *(volatile int*)&sel->tie;
   __syncthreads();
   if (!sGo) return;
-  if (blockIdx.x == 0) exact_select(a, 1, smem);
+  if (blockIdx.x == 0) {
+    __shared__ ExactOut eo;
+    exact_select(a, 1, smem, *(volatile long long*)&sel->n_tie, *(volatile int*)&sel->tie_overflow != 0,
+                 sel->need, sel->prefix, true, &eo);
+  }
   if (!grid_sync(a)) return;
-  const long long m0 = *(volatile long long*)&sel->n_cand;
+  const long long m0 = *(volatile long long*)&sel->n_tie;
   const long long m = m0 < a.ws.max_n ? m0 : a.ws.max_n;
   const long long nslots = (long long)ns * a.in->nnz;
   const unsigned long long tk = *(volatile unsigned long long*)&sel->t_key;
