@@ -243,7 +243,7 @@ def run_ours(a, rank, world, dist):
     roofline = None
     kernels = None
     if not a.no_profile:
-        roofline, kernels = profile_step(a, circ, L, _native, BASS, torch)
+        roofline, kernels = profile_step(a, circ, L, _native, BASS, torch, 1e3 * t_total / a.steps)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -266,7 +266,7 @@ def run_ours(a, rank, world, dist):
         print(json.dumps(line), flush=True)
 
 
-def profile_step(a, circ, L, nat, BASS, torch):
+def profile_step(a, circ, L, nat, BASS, torch, step_ms):
     """One extra step with per-launch CUDA events and per-kernel entry counters."""
     import numpy as np
     L.bass_profile_enable(1)
@@ -302,9 +302,20 @@ def profile_step(a, circ, L, nat, BASS, torch):
         tj = json.load(open(tfile))
         if nat.SLOT_NAMES[dom] in tj:
             traffic = tj[nat.SLOT_NAMES[dom]] * per_launch_bytes / 24
+    # the whole simulate call: every gate / rotation / truncation reads its
+    # input once and writes its output once (24 B per entry each way), over
+    # the timed step's duration (RDMs, selection, partitions all included)
+    kinds = (0, 1, 2, 4)  # gate1, rot1, gate2, plain; the 2-qubit gate's first pass is overhead
+    step_bytes = 24 * (sum(int(c["prof_in"][k * 5 + 0]) for k in kinds) +
+                       sum(int(c["prof_out"][k * 5 + 3]) for k in kinds))
+    step_gbs = step_bytes / (step_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": nat.SLOT_NAMES[dom], "achieved": round(achieved, 1), "peak": peak,
             "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "bytes_per_launch": per_launch_bytes,
+            "whole_step": {"achieved": round(step_gbs, 1), "frac": round(step_gbs / peak, 4),
+                           "bytes_per_step": step_bytes,
+                           "note": "24 B per entry read + 24 B per entry written by every gate, rotation step "
+                                   "and truncation, over the timed step"},
             "note": "algorithmic bytes = 24 B per entry read + 24 B per entry written; timing from a "
                     "profiled step (CUDA events around each launch on its stream)"}
     return roof, kernels[:12]
