@@ -240,6 +240,41 @@ __device__ __forceinline__ long long warp_first_false(long long lo, long long hi
   return lo + __popc(m);
 }
 
+// Three lower bounds on one sorted array in lockstep: lo[k] becomes the first
+// index in [lo[k], hi[k]) with keys[i] >= thr[k] (hi[k] if none).  Every round
+// each lane probes one position of every unfinished search, so the three
+// chains of dependent loads overlap.  Called by all 32 lanes of a warp.
+__device__ __forceinline__ void warp_lower_bound3(const uint64_t* keys, long long (&lo)[3], long long (&hi)[3],
+                                                  const uint64_t (&thr)[3]) {
+  const int lane = threadIdx.x & 31;
+  while (hi[0] - lo[0] > 32 || hi[1] - lo[1] > 32 || hi[2] - lo[2] > 32) {
+    bool tk[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const long long span = hi[k] - lo[k];
+      tk[k] = span > 32 && keys[lo[k] + (span * (lane + 1)) / 33] < thr[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const long long span = hi[k] - lo[k];
+      const unsigned m = __ballot_sync(0xffffffffu, tk[k]);
+      if (span > 32) {
+        const int c = __popc(m);
+        const long long nlo = (c == 0) ? lo[k] : lo[k] + (span * c) / 33 + 1;
+        const long long nhi = (c == 32) ? hi[k] : lo[k] + (span * (c + 1)) / 33;
+        lo[k] = nlo;
+        hi[k] = nhi;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const long long p = lo[k] + lane;
+    const bool t = p < hi[k] && keys[p] < thr[k];
+    lo[k] += __popc(__ballot_sync(0xffffffffu, t));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // decoupled look-back (exclusive prefix of per-tile counts)
 // status word: bits 62-63 flag (1 aggregate, 2 inclusive), bits 0-61 value

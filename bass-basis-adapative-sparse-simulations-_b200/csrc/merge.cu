@@ -14,13 +14,14 @@
 //   k_tile        loads a tile's (at most five) contiguous input segments,
 //                 splits them by bit t and merges them in shared memory, then
 //                 evaluates every group (gate / rotation / permutation / RDM
-//                 moments) and, depending on the pass, histograms the
-//                 children's |a|^2, gathers top-k boundary candidates, or
-//                 writes the surviving children in order (decoupled look-back);
-//   k_select*     radix select of the top-k threshold (13-bit digits on the
-//                 IEEE bits of |a|^2, then an exact (|a|^2 desc, key asc)
-//                 ordering of the boundary candidates);
-//   finalize_op   (last CTA of the write pass) output descriptor (count, new
+//                 moments); the evaluation pass stages every child (|a|^2 bit
+//                 pattern, key, amplitude) at its slot index;
+//   k_select_coop cooperative selection: radix select of the top-k threshold
+//                 on the IEEE bits of |a|^2 (13-bit digits, then an exact
+//                 (|a|^2 desc, key asc) ordering of the boundary candidates),
+//                 survivors per tile, exact sums, rotation decision, tile scan;
+//   k_compact     copies the surviving staged children to their tile's offset;
+//   finalize_op   (last CTA of the write step) output descriptor (count, new
 //                 bit order, pending renormalisation) and the gamma /
 //                 truncation bookkeeping.
 //
@@ -85,9 +86,12 @@ __global__ void k_partition(OpArgs a, int kind) {
       const uint64_t mid_key = lo_key | (1ULL << t);
       const uint64_t hi_key = lo_key + (2ULL << t);
       const bool hi_ovf = hi_key <= lo_key;
-      long long s = warp_first_false(0, P + 1, [&](long long i) { return keys[i] < lo_key; });
-      long long mid = warp_first_false(s, n, [&](long long i) { return keys[i] < mid_key; });
-      long long e = hi_ovf ? n : warp_first_false(P, n, [&](long long i) { return keys[i] < hi_key; });
+      // block start, run split and block end in one lockstep search
+      long long lo3[3] = {0, ((y >> t) & 1ULL) ? 0 : P + 1, hi_ovf ? n : P + 1};
+      long long hi3[3] = {P + 1, ((y >> t) & 1ULL) ? P + 1 : n, n};
+      const uint64_t thr3[3] = {lo_key, mid_key, hi_key};
+      warp_lower_bound3(keys, lo3, hi3, thr3);
+      const long long s = lo3[0], mid = lo3[1], e = lo3[2];
       const long long d = P - s, len0 = mid - s, len1 = e - mid;
       long long lo = d - len1 > 0 ? d - len1 : 0;
       long long hi = d < len0 ? d : len0;
@@ -96,12 +100,23 @@ __global__ void k_partition(OpArgs a, int kind) {
       });
       long long j = d - i;
       if (kind != K_PERM) {
-        uint64_t z0 = (i < len0) ? zmove(keys[s + i], t, gb) : ~0ULL;
-        uint64_t z1 = (j < len1) ? zmove(keys[mid + j], t, gb) : ~0ULL;
-        uint64_t gid = (z0 < z1 ? z0 : z1) >> sh;
+        // back the boundary off to the start of its group: the two entries
+        // at the split and the two before it in each run, fetched at once
+        long long idx = -1;
+        if (lane == 0 && i < len0) idx = s + i;
+        if (lane == 1 && j < len1) idx = mid + j;
+        if (lane == 2 && i >= 1) idx = s + i - 1;
+        if (lane == 3 && i >= 2) idx = s + i - 2;
+        if (lane == 4 && j >= 1) idx = mid + j - 1;
+        if (lane == 5 && j >= 2) idx = mid + j - 2;
+        const uint64_t zv = (idx >= 0) ? zmove(keys[idx], t, gb) : ~0ULL;
+        const uint64_t z0 = __shfl_sync(0xffffffffu, zv, 0), z1 = __shfl_sync(0xffffffffu, zv, 1);
+        const uint64_t a1 = __shfl_sync(0xffffffffu, zv, 2), a2 = __shfl_sync(0xffffffffu, zv, 3);
+        const uint64_t c1 = __shfl_sync(0xffffffffu, zv, 4), c2 = __shfl_sync(0xffffffffu, zv, 5);
+        const uint64_t gid = (z0 < z1 ? z0 : z1) >> sh;
         int b0 = 0, b1 = 0;
-        while (b0 < 2 && i - b0 - 1 >= 0 && (zmove(keys[s + i - b0 - 1], t, gb) >> sh) == gid) ++b0;
-        while (b1 < 2 && j - b1 - 1 >= 0 && (zmove(keys[mid + j - b1 - 1], t, gb) >> sh) == gid) ++b1;
+        if (i >= 1 && (a1 >> sh) == gid) b0 = (i >= 2 && (a2 >> sh) == gid) ? 2 : 1;
+        if (j >= 1 && (c1 >> sh) == gid) b1 = (j >= 2 && (c2 >> sh) == gid) ? 2 : 1;
         i -= b0;
         j -= b1;
       }
@@ -228,7 +243,7 @@ constexpr unsigned long long kSlotKeptTie = 0x7FFFFFFFFFFFFFFEULL;
 
 // Does the child with this slot survive the selection?  (T, incl) = (t_bits,
 // t_key == ~0) when truncating, (0, true) otherwise; ties settled by key were
-// rewritten to kSlotKeptTie / 0 by k_tie_coop.
+// rewritten to kSlotKeptTie / 0 by the selection.
 __device__ __forceinline__ bool slot_kept(unsigned long long bits, unsigned long long T, bool incl) {
   return bits != ~0ULL && (bits > T || (incl && bits == T));
 }
@@ -304,10 +319,10 @@ __device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int
 // the tile kernel
 // ---------------------------------------------------------------------------
 // Passes: P_HIST (evaluate every child once: its |a|^2 bits go to the slot
-// array, plus the child count), P_GATHER (only on an exact tie at the
-// threshold: collect (slot index, true key) of the tied children), P_WRITE
-// (the kept-children mask of every group from the slot array, then evaluate
-// and write the groups that keep any, in order), P_RDM (per-qubit moments).
+// array, its key and amplitude to the staging arrays at the same index, plus
+// the child count), P_WRITE (the first pass of a 2-qubit gate, one child per
+// entry, and the compaction after a diagonal 1-qubit gate), P_RDM (per-qubit
+// moments).
 template <int KIND, int PASS>
 __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -327,7 +342,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
   if (tid < 16) sG[tid] = a.G[tid];
   if (tid == 0) S = *a.ws.sel;
   __syncthreads();
-  if (PASS == P_GATHER && S.stage != 4) return;
   if (KIND == K_IDENT && a.guard && S.pad == 0) return;
   // a rejected rotation candidate is not written (the descriptor still is)
   const bool skip = PASS == P_WRITE && S.skip_write;
@@ -669,28 +683,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
             *reinterpret_cast<ulonglong2*>(slots + (long long)NS * p + c) = make_ulonglong2(sb[c], sb[c + 1]);
         }
       }
-    } else if (PASS == P_GATHER) {
-      constexpr int MC = KindTraits<KIND>::kMaxChildren;
-      uint64_t kb;
-      double2 ca[MC];
-      for (int p = tid; p < E; p += kThreads) {
-        const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
-#pragma unroll
-        for (int c = 0; c < MC; ++c) {
-          if (!((cm >> c) & 1u)) continue;
-          const uint64_t bits = (uint64_t)__double_as_longlong(prob(ca[c]));
-          if (bits == S.prefix) {
-            const unsigned long long slot =
-                atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws.sel->n_tie), 1ULL);
-            if ((long long)slot < a.ws.max_n) {
-              a.ws.cand_bits[slot] = (unsigned long long)(NS * (sZstart + p) + c);  // its slot index
-              a.ws.cand_key[slot] = true_key(kb | (uint64_t)c, H.qat_out, 64);
-            } else {
-              a.ws.sel->tie_overflow = 1;
-            }
-          }
-        }
-      }
     }
     __syncthreads();
   }
@@ -740,10 +732,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
 //   4. the last block to finish step 3: the exact sums, the rotation
 //      decision, and an exclusive scan of the tile counts (each tile of the
 //      write step then knows its base).
-// An exact tie at the threshold (equal bit patterns straddling rank k) stops
-// it after step 2; the tied children's keys are then collected by the tile
-// kernel's P_GATHER pass and k_tie_coop settles the tie by key and runs
-// steps 3-4.  The grid barrier is a counter and a generation word in the
+// An exact tie at the threshold (equal bit patterns straddling rank k) is
+// settled inside step 2: the tied children's true keys are read from the
+// staged keys, the smallest `need` of them survive, and their slots are
+// rewritten as kept / dropped before step 3.  The grid barrier is a counter and a generation word in the
 // workspace with a bounded spin (BASS_ERR_WAIT, then every block returns).
 constexpr int kSelThreads = 512;
 
@@ -1397,14 +1389,70 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
         } else {
           if (blockIdx.x == 0) exact_select(a, 0, smem, mc, sOvf != 0, need2, pre, true, &eo);
           if (!grid_sync(a)) return;
-          if (tid == 0) {
-            eo.stage = *(volatile int*)&sel->stage;
-            eo.t_bits = *(volatile unsigned long long*)&sel->t_bits;
+          if (tid == 0) {  // block 0's result, for every block
+            volatile SelState* vs = sel;
+            eo.stage = vs->stage;
+            eo.t_bits = vs->t_bits;
+            eo.prefix = vs->prefix;
+            eo.need = vs->need;
           }
           __syncthreads();
         }
-        if (eo.stage == 4) return;  // exact tie: P_GATHER and k_tie_coop continue
-        T = eo.t_bits;
+        if (eo.stage != 4) {
+          T = eo.t_bits;
+        } else {
+          // An exact tie at T: the survivors among the children at T are the
+          // `need` smallest true keys.  Their keys come from the staging
+          // array (new physical keys, mapped back through the output order).
+          if (!grid_sync(a)) return;  // every block is done with the level-2 candidates
+          __shared__ int8_t sQat[64];
+          if (tid == 0) out_order(a.in, kind, kind == K_IDENT ? 0 : a.in->pos[a.q], a.gb, sQat);
+          __syncthreads();
+          const unsigned long long Tt = eo.prefix;
+          scan_slots(slots, nslots, [&](unsigned long long bits, long long i) {
+            if (bits == Tt) {
+              const unsigned long long k =
+                  atomicAdd(reinterpret_cast<unsigned long long*>(&sel->n_tie), 1ULL);
+              if ((long long)k < a.ws.max_n) {
+                a.ws.cand_bits[k] = (unsigned long long)i;
+                a.ws.cand_key[k] = true_key(a.ws.stage_keys[i], sQat, 64);
+              } else {
+                sel->tie_overflow = 1;
+              }
+            }
+          });
+          if (!grid_sync(a)) return;
+          __shared__ ExactOut eo2;
+          __shared__ long long sMt;
+          __shared__ int sOvt;
+          if (tid == 0) {
+            sMt = *(volatile long long*)&sel->n_tie;
+            sOvt = *(volatile int*)&sel->tie_overflow;
+          }
+          __syncthreads();
+          const long long mt = sMt;
+          if (mt <= kCandSmem && !sOvt) {
+            exact_select(a, 1, smem, mt, false, eo.need, Tt, blockIdx.x == 0, &eo2);
+          } else {
+            if (blockIdx.x == 0) exact_select(a, 1, smem, mt, sOvt != 0, eo.need, Tt, true, &eo2);
+            if (!grid_sync(a)) return;
+            if (tid == 0) eo2.t_key = *(volatile unsigned long long*)&sel->t_key;
+            __syncthreads();
+          }
+          T = Tt;
+          tkey = eo2.t_key;
+          incl = false;
+          // rewrite the tied slots as kept / dropped, so that the survivors
+          // are decided by the slot alone from here on
+          unsigned long long* wslots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys);
+          const long long mm = mt < a.ws.max_n ? mt : a.ws.max_n;
+          for (long long k = (long long)blockIdx.x * blockDim.x + tid; k < mm;
+               k += (long long)gridDim.x * blockDim.x) {
+            const unsigned long long i = __ldcg(a.ws.cand_bits + k);
+            if ((long long)i < nslots) wslots[i] = (__ldcg(a.ws.cand_key + k) <= tkey) ? kSlotKeptTie : 0ULL;
+          }
+          if (!grid_sync(a)) return;
+        }
       }
     }
   }
@@ -1419,44 +1467,6 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
   // 3. survivors per tile and exact sums
   count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, sCnt);
   // 4. sums, decision, tile offsets
-  finish_by_last_block(a, kind, mode, j, trace, sRed);
-}
-
-// The exact-tie continuation (only when k_select_coop stopped at stage 4 and
-// the P_GATHER pass has collected the tied children): settle the tie by key,
-// rewrite the tied slots as kept (kSlotKeptTie) or dropped (0), then steps 3-4.
-template <bool P2>
-__global__ void __launch_bounds__(kSelThreads) k_tie_coop(OpArgs a, int ns, int kind, int mode, int j,
-                                                           int trace) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ i128 sRed[3 * (kSelThreads / 32)];
-  __shared__ int sCnt[kSelThreads / 32];
-  __shared__ int sGo;
-  SelState* sel = a.ws.sel;
-  // sel->tie is set only by the selection's exact step and is not changed in
-  // this kernel, so every block takes the same branch
-  if (threadIdx.x == 0) sGo = *(volatile int*)&sel->tie;
-  __syncthreads();
-  if (!sGo) return;
-  if (blockIdx.x == 0) {
-    __shared__ ExactOut eo;
-    exact_select(a, 1, smem, *(volatile long long*)&sel->n_tie, *(volatile int*)&sel->tie_overflow != 0,
-                 sel->need, sel->prefix, true, &eo);
-  }
-  if (!grid_sync(a)) return;
-  const long long m0 = *(volatile long long*)&sel->n_tie;
-  const long long m = m0 < a.ws.max_n ? m0 : a.ws.max_n;
-  const long long nslots = (long long)ns * a.in->nnz;
-  const unsigned long long tk = *(volatile unsigned long long*)&sel->t_key;
-  const unsigned long long T = *(volatile unsigned long long*)&sel->t_bits;
-  unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys);
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-       k += (long long)gridDim.x * blockDim.x) {
-    const unsigned long long i = __ldcg(a.ws.cand_bits + k);
-    if ((long long)i < nslots) slots[i] = (__ldcg(a.ws.cand_key + k) <= tk) ? kSlotKeptTie : 0ULL;
-  }
-  if (!grid_sync(a)) return;
-  count_phase<P2>(a, ns, kind, T, false, true, sRed, sCnt);
   finish_by_last_block(a, kind, mode, j, trace, sRed);
 }
 
@@ -1640,42 +1650,34 @@ cudaError_t zero_small(const WsView& ws, cudaStream_t s) {
   return cudaMemsetAsync(ws.counters, 0, bytes, s);
 }
 
-// Cooperative launch of the selection (tie = false) or of its exact-tie
-// continuation (tie = true); grid = every co-resident block.
+// Cooperative launch of the selection; grid = every co-resident block.
 template <bool P2>
-static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace, bool tie,
+static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace,
                                    cudaStream_t s) {
   const size_t smem = (size_t)kCandSmem * 16;
-  static int grid[2] = {0, 0};
-  int& g = grid[tie ? 1 : 0];
-  if (g == 0) {
-    const void* f = tie ? (const void*)k_tie_coop<P2> : (const void*)k_select_coop<P2>;
+  static int grid = 0;
+  if (grid == 0) {
+    const void* f = (const void*)k_select_coop<P2>;
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int occ = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kSelThreads, smem);
     if (e != cudaSuccess) return e;
     if (occ < 1) return cudaErrorInvalidConfiguration;
-    g = device().sms * occ;
-    if (g > 1024) g = 1024;  // per-CTA partials
+    grid = device().sms * occ;
+    if (grid > 1024) grid = 1024;  // per-CTA partials
   }
   a.prof = prof_on() ? 1 : 0;
-  dim3 grd(g), blk(kSelThreads);
+  dim3 grd(grid), blk(kSelThreads);
   cudaError_t e = cudaSuccess;
-  if (tie) {
-    void* args[] = {&a, &ns, &kind, &mode, &j, &trace};
-    KLAUNCH(S_SELECT_EXACT, s, e = cudaLaunchCooperativeKernel((const void*)k_tie_coop<P2>, grd, blk, args, smem, s));
-  } else {
-    void* args[] = {&a, &ns, &kind, &gh, &mode, &j, &trace};
-    KLAUNCH(S_SELECT1, s, e = cudaLaunchCooperativeKernel((const void*)k_select_coop<P2>, grd, blk, args, smem, s));
-  }
+  void* args[] = {&a, &ns, &kind, &gh, &mode, &j, &trace};
+  KLAUNCH(S_SELECT1, s, e = cudaLaunchCooperativeKernel((const void*)k_select_coop<P2>, grd, blk, args, smem, s));
   return e;
 }
 
-static cudaError_t launch_select(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace, bool tie,
-                                 cudaStream_t s) {
-  return mode == 1 ? launch_select_t<true>(a, ns, kind, gh, mode, j, trace, tie, s)
-                   : launch_select_t<false>(a, ns, kind, gh, mode, j, trace, tie, s);
+static cudaError_t launch_select(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace, cudaStream_t s) {
+  return mode == 1 ? launch_select_t<true>(a, ns, kind, gh, mode, j, trace, s)
+                   : launch_select_t<false>(a, ns, kind, gh, mode, j, trace, s);
 }
 
 template <int KIND>
@@ -1692,9 +1694,7 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
     constexpr int ns = slots_per_entry(KIND);
     int gh = 0;
     if ((e = launch_tile<KIND, P_HIST>(a, 0, s, &gh)) != cudaSuccess) return e;
-    if ((e = launch_select(a, ns, KIND, gh, fin_mode, j, tr.trace, false, s)) != cudaSuccess) return e;
-    if ((e = launch_tile<KIND, P_GATHER>(a, 2, s, nullptr)) != cudaSuccess) return e;
-    if ((e = launch_select(a, ns, KIND, gh, fin_mode, j, tr.trace, true, s)) != cudaSuccess) return e;
+    if ((e = launch_select(a, ns, KIND, gh, fin_mode, j, tr.trace, s)) != cudaSuccess) return e;
   }
   a.fin = 1;
   a.fin_mode = fin_mode;
