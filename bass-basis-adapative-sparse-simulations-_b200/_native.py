@@ -44,6 +44,11 @@ SLOT_NAMES = [f"k_tile<{k},{p}>" for k in KINDS for p in PASSES] + [
     "k_partition", "k_select_coop", "k_select2", "k_tie_coop", "k_finalize", "reductions", "k_fingerprint",
     "k_phase2q", "k_phase1q", "k_rdm_final", "radix_sort", "merge_runs", "bookkeeping", "k_slot_hist<1>",
     "k_slot_hist<2>", "k_slot_gather", "k_tile_counts"] + [f"slot{i}" for i in range(47, 48)]
+# the write step of gates, rotations and truncations is k_compact, counted in the write slot
+SLOT_NAMES[0 * 5 + 3] = "k_compact<gate1>"
+SLOT_NAMES[1 * 5 + 3] = "k_compact<rot1>"
+SLOT_NAMES[2 * 5 + 3] = "k_compact<gate2>"
+SLOT_NAMES[4 * 5 + 3] = "k_compact<plain>"
 
 
 class Trunc(ctypes.Structure):
