@@ -968,7 +968,51 @@ __device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem, lon
   const int tid = threadIdx.x;
   __shared__ unsigned long long sT;
   __shared__ long long sGt, sEq;
-  if (m <= kCandSmem) {
+  if (m <= kRankMax) {
+    // few candidates: the rank of each is the number that rank above it
+    for (long long i = tid; i < m; i += blockDim.x) {
+      sb[i] = (mode == 1) ? 1ULL : __ldcg(a.ws.cand_bits + i);
+      sk[i] = __ldcg(a.ws.cand_key + i);
+    }
+    __shared__ int sSel, sGtI, sEqI;
+    if (tid == 0) { sSel = 0; sGtI = 0; sEqI = 0; }
+    __syncthreads();
+    const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
+    for (long long i = tid; i < m; i += blockDim.x) {
+      long long rank = 0;
+      for (long long jx = 0; jx < m; ++jx) rank += better(sb[jx], sk[jx], sb[i], sk[i]);
+      if (rank == r) sSel = (int)i;
+    }
+    __syncthreads();
+    const unsigned long long Tsel = sb[sSel];
+    if (mode == 0) {
+      for (long long i = tid; i < m; i += blockDim.x) {
+        if (sb[i] > Tsel) atomicAdd(&sGtI, 1);
+        else if (sb[i] == Tsel) atomicAdd(&sEqI, 1);
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      if (mode == 1) {
+        out->stage = 3;
+        out->t_bits = sPre;
+        out->t_key = sk[sSel];
+        if (writer) {
+          sel->t_bits = sPre;
+          sel->t_key = sk[sSel];
+          sel->stage = 3;
+        }
+      } else {
+        sT = Tsel;
+        sGt = sGtI;
+        sEq = sEqI;
+      }
+    }
+    if (mode == 1) {
+      __syncthreads();
+      return;
+    }
+  } else if (m <= kCandSmem) {
     sort_candidates(sb, sk, m, a.ws, mode == 1);
     const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
     if (mode == 1) {
