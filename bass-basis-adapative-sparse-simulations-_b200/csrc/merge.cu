@@ -1147,9 +1147,12 @@ __device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem, lon
 
 // The tile holding Z position z (tiles start at the partition's adjusted
 // positions P'_b <= b * kStep; plain tiles every kTile positions).
+// positions fit 32 bits (every op's count is below 2^31), so the divisions
+// are 32-bit divisions by constants
 __device__ __forceinline__ long long tile_of(long long z, int kind, const long long* part) {
-  if (kind == K_IDENT) return z / kTile;
-  const long long b0 = z / kStep;
+  const unsigned zu = (unsigned)z;
+  if (kind == K_IDENT) return (long long)(zu / (unsigned)kTile);
+  const long long b0 = (long long)(zu / (unsigned)kStep);
   return (z >= part[(b0 + 1) * 6]) ? b0 + 1 : b0;
 }
 
@@ -1168,6 +1171,7 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
   const long long nslots = (long long)ns * n;
   const bool sums = P2 || trunc;
   const bool want_total = trunc && !P2;  // gamma bookkeeping of plain truncations only
+  const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;  // slots per entry: 1, 2 or 4
   const int lane = threadIdx.x & 31;
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
   const long long* part = a.ws.part;
@@ -1210,8 +1214,8 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
     // survivors per tile
     const bool live = c < nchunk;
     const long long last = (s0 + 7 < nslots ? s0 + 7 : nslots - 1);
-    const long long t0 = live ? tile_of(s0 / ns, kind, part) : -1;
-    const long long t1 = live ? tile_of(last / ns, kind, part) : -1;
+    const long long t0 = live ? tile_of(s0 >> lns, kind, part) : -1;
+    const long long t1 = live ? tile_of(last >> lns, kind, part) : -1;
     const long long w0 = __shfl_sync(0xffffffffu, t0, 0);
     const bool uniform = __all_sync(0xffffffffu, !live || (t0 == w0 && t1 == w0));
     if (uniform) {
@@ -1222,7 +1226,7 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
     } else if (live) {
       for (int u = 0; u < 8; ++u) {
         if (!((km >> u) & 1u)) continue;
-        const long long tb = (u == 0) ? t0 : tile_of((s0 + u) / ns, kind, part);
+        const long long tb = (u == 0) ? t0 : tile_of((s0 + u) >> lns, kind, part);
         atomicAdd(reinterpret_cast<unsigned long long*>(a.ws.status + tb), 1ULL);
       }
     }
@@ -1352,7 +1356,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
   const long long n = a.in->nnz;
   const long long nslots = (long long)ns * n;
   const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
-  if (nslots > a.ws.max_n || ntiles > a.ws.max_tiles) {  // uniform: every block returns
+  if (nslots > a.ws.max_n || ntiles > a.ws.max_tiles || n >= (1LL << 31)) {  // uniform: every block returns
     if (blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
     return;
   }
