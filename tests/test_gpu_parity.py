@@ -159,6 +159,29 @@ def test_topk_large_ties(B, orc):
     assert np.array_equal(st.x, np.sort(xo))
 
 
+@pytest.mark.parametrize("n_tied", [7, 100, 2000])
+def test_topk_ties_at_threshold(B, orc, n_tied):
+    """A run of equal |a|^2 straddling rank k: the survivors among them are the
+    smallest keys.  Tie sizes cover the counting (<= 256), sorting (<= 4096)
+    and radix paths of the exact candidate step."""
+    from bass_b200 import _native
+    rng = np.random.default_rng(9 + n_tied)
+    N, n = 24, 30000
+    x = np.unique(rng.integers(0, 2 ** N, size=2 * n, dtype=np.uint64))[:n]
+    rng.shuffle(x)
+    a = (rng.uniform(0.5, 1.0, n) + 1j * rng.uniform(-0.5, 0.5, n)) / 100.0
+    tied = np.full(n_tied, 0.0065 + 0.0j)
+    big = np.abs(a) ** 2 > np.abs(tied[0]) ** 2
+    k = int(big.sum()) + n_tied // 2          # the cut falls inside the tied run
+    idx = np.flatnonzero(~big)[:n_tied]
+    a[idx] = tied
+    st = gpu_state(B, N, x, a)
+    st._topk(_native.trunc(k, k))
+    xo, ao, _, _ = orc.select_topk(x, a, k)
+    assert st.nnz == k
+    assert np.array_equal(st.x, np.sort(xo))
+
+
 def test_rdm_exact(B, orc):
     rng = np.random.default_rng(3)
     for N, n in [(12, 300), (40, 50000)]:
