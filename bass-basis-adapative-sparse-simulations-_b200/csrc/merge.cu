@@ -745,8 +745,10 @@ __device__ bool grid_sync(const OpArgs& a) {
   __shared__ int sOk;
   __syncthreads();
   if (threadIdx.x == 0) {
+    // arrival counter and generation word on separate cache lines, so that
+    // the waiting blocks' polling does not slow down the arrivals
     unsigned long long* cnt = reinterpret_cast<unsigned long long*>(a.ws.counters) + 60;
-    unsigned long long* gen = cnt + 1;
+    unsigned long long* gen = reinterpret_cast<unsigned long long*>(a.ws.counters) + 32;
     const unsigned long long g = ld_acquire(gen);
     __threadfence();
     const unsigned long long arrived = atomicAdd(cnt, 1ULL);
@@ -763,6 +765,7 @@ __device__ bool grid_sync(const OpArgs& a) {
           ok = 0;
           break;
         }
+        __nanosleep(32);
       }
     }
     __threadfence();
