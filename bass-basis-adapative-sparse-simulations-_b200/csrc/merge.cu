@@ -172,14 +172,28 @@ struct KindTraits {
 // start a group); child o has the new physical key base | o and amplitude
 // ca[o].  Within a group, entries are in ascending local index, so the sums
 // run over the local index in ascending order.
+// The tile's amplitudes as the evaluation sees them: stored in load order,
+// read at Z position p through the merge's permutation (identity when there
+// is none), with the state's pending renormalisation applied.
+struct AmpView {
+  const double2* sA;
+  const uint16_t* sP;  // Z position -> load position, or nullptr
+  double r0, r1;
+  bool scaled;
+  __device__ __forceinline__ double2 operator()(int p) const {
+    const double2 v = sA[sP ? (int)sP[p] : p];
+    return scaled ? scale_load(v, r0, r1) : v;
+  }
+};
+
 template <int KIND>
-__device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t* sZ, const double2* sA, int gb,
+__device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t* sZ, const AmpView& sA, int gb,
                                                    const double2* sG, int drop_zero, uint64_t* base,
                                                    double2* ca) {
   constexpr int NC = KindTraits<KIND>::kMaxChildren;
   const uint64_t z = sZ[p];
   if (KIND == K_PERM || KIND == K_IDENT) {
-    const double2 v = sA[p];
+    const double2 v = sA(p);
     if (KIND == K_IDENT && drop_zero && !cnz(v)) return 0u;
     *base = z;
     ca[0] = v;
@@ -196,7 +210,7 @@ __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t*
     const uint64_t zr = (p + r < E) ? sZ[p + r] : ~0ULL;
     const bool in = (p + r < E) && (zr >> sh) == gid;
     lr[r] = in ? (int)(zr & ((1u << sh) - 1)) : -1;
-    ar[r] = in ? sA[p + r] : make_double2(0.0, 0.0);
+    ar[r] = in ? sA(p + r) : make_double2(0.0, 0.0);
   }
   unsigned mask = 0;
   if (KIND == K_GATE1 || KIND == K_GATE2) {
@@ -330,6 +344,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
   uint64_t* sZ = reinterpret_cast<uint64_t*>(sA + kTilePad);
   uint64_t* sK = sZ + kTilePad;
   uint16_t* sIdx = reinterpret_cast<uint16_t*>(sK + kTilePad);
+  uint16_t* sPerm = reinterpret_cast<uint16_t*>(sK);  // after the merge (sK is free then)
   __shared__ Hdr H;
   __shared__ SelState S;
   __shared__ long long sItem, sBase, sZstart;
@@ -443,10 +458,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
       asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
-    if (KIND == K_IDENT && scaled) {
-      for (int e = tid; e < E; e += kThreads) sA[e] = scale_load(sA[e], H.r0, H.r1);
-      __syncthreads();
-    }
 
     // ---- Z order: stable split by the target bit, merge, write back --------
     // The split moves the Z keys (zmove of the loaded keys) into sK, bit-clear
@@ -518,24 +529,21 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
           z1 = (j < n1) ? K1[j] : ~0ULL;
         }
       }
-      double2 ra[kPerThread];
+      uint16_t rp[kPerThread];
 #pragma unroll
-      for (int k = 0; k < kPerThread; ++k) {
-        if (d + k < E) {
-          const double2 v = sA[sIdx[rs[k]]];
-          ra[k] = scaled ? scale_load(v, H.r0, H.r1) : v;
-        }
-      }
+      for (int k = 0; k < kPerThread; ++k) rp[k] = (d + k < E) ? sIdx[rs[k]] : 0;
       __syncthreads();
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
         if (d + k < E) {
           sZ[d + k] = rz[k];
-          sA[d + k] = ra[k];
+          sPerm[d + k] = rp[k];  // the amplitudes stay where they were loaded
         }
       }
       __syncthreads();
     }
+
+    const AmpView amp{sA, KIND == K_IDENT ? nullptr : sPerm, H.r0, H.r1, scaled};
 
     // ---- evaluate ------------------------------------------------------------
     // Round r gives position r * kThreads + tid to thread tid, so neighbouring
@@ -546,11 +554,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
         const uint64_t z = sZ[p];
         const uint64_t gid = z >> 1;
         if (p > 0 && (sZ[p - 1] >> 1) == gid) continue;
-        const double2 x0 = sA[p];
+        const double2 x0 = amp(p);
         if ((z & 1ULL) == 0) {
           v[0] += fx_from(prob(x0));
           if (p + 1 < E && (sZ[p + 1] >> 1) == gid) {
-            const double2 x1 = sA[p + 1];
+            const double2 x1 = amp(p + 1);
             v[1] += fx_from(prob(x1));
             const double2 c = cmul(x0, make_double2(x1.x, -x1.y));
             v[2] += fx_from(c.x);
@@ -574,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
       uint64_t kb;
       double2 ca[MC];
       uint16_t* sOff = sIdx;                              // free after the merge
-      uint8_t* sMask = reinterpret_cast<uint8_t*>(sK);    // free after the merge
+      uint8_t* sMask = reinterpret_cast<uint8_t*>(sK) + 2 * kTilePad;  // after sPerm
       const int wmode = a.write_mode;
       // (a) kept-children mask per position
       for (int p = tid; p < E; p += kThreads) {
@@ -582,7 +590,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
         if (wmode == 2) {
           mk = 1u;
         } else {
-          const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+          const unsigned cm = group_children<KIND>(p, E, sZ, amp, gb, sG, a.drop_zero, &kb, ca);
           if ((cm & 1u) && keep_child((uint64_t)__double_as_longlong(prob(ca[0])), kb, S, H.qat_out)) mk = 1u;
         }
         sMask[p] = (uint8_t)mk;
@@ -630,7 +638,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
           const unsigned mk = sMask[p];
           if (!mk) continue;
           long long o = sBase + sOff[p];
-          group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+          group_children<KIND>(p, E, sZ, amp, gb, sG, a.drop_zero, &kb, ca);
 #pragma unroll
           for (int c = 0; c < MC; ++c) {
             if ((mk >> c) & 1u) {
@@ -651,7 +659,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
       uint64_t* skeys = a.ws.stage_keys + NS * sZstart;
       double2* samps = a.ws.tmp_amps + NS * sZstart;
       for (int p = tid; p < E; p += kThreads) {
-        const unsigned cm = group_children<KIND>(p, E, sZ, sA, gb, sG, a.drop_zero, &kb, ca);
+        const unsigned cm = group_children<KIND>(p, E, sZ, amp, gb, sG, a.drop_zero, &kb, ca);
         unsigned long long sb[NS];
 #pragma unroll
         for (int c = 0; c < NS; ++c) {
