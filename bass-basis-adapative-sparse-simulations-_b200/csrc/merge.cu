@@ -338,13 +338,15 @@ __device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int
 // entry, and the compaction after a diagonal 1-qubit gate), P_RDM (per-qubit
 // moments).
 template <int KIND, int PASS>
-__global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   double2* sA = reinterpret_cast<double2*>(smem);
   uint64_t* sZ = reinterpret_cast<uint64_t*>(sA + kTilePad);
-  uint64_t* sK = sZ + kTilePad;
-  uint16_t* sIdx = reinterpret_cast<uint16_t*>(sK + kTilePad);
-  uint16_t* sPerm = reinterpret_cast<uint16_t*>(sK);  // after the merge (sK is free then)
+  uint16_t* sIdx = reinterpret_cast<uint16_t*>(sZ + kTilePad);
+  uint16_t* sPerm = sIdx;  // after the merge: Z position -> load position
+  // write pass only: per-position offsets and kept masks
+  uint16_t* sOff = sIdx + kTilePad;
+  uint8_t* sMask = reinterpret_cast<uint8_t*>(sOff + kTilePad);
   __shared__ Hdr H;
   __shared__ SelState S;
   __shared__ long long sItem, sBase, sZstart;
@@ -460,9 +462,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
     __syncthreads();
 
     // ---- Z order: stable split by the target bit, merge, write back --------
-    // The split moves the Z keys (zmove of the loaded keys) into sK, bit-clear
-    // run first, with their load positions in sIdx; the merge then reads keys
-    // from sK alone and gathers the amplitudes once at the end.
+    // The split rewrites the Z keys (zmove of the loaded keys) in place, bit-
+    // clear run first, with their load positions in sIdx; the merge reads the
+    // two runs and leaves the Z-ordered keys in sZ and, in sIdx, the load
+    // position of each Z position (the amplitudes are not moved).
     if (KIND != K_IDENT) {
       const int lane = tid & 31, w = tid >> 5;
       const unsigned lt = (1u << lane) - 1;
@@ -494,7 +497,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
         const unsigned ones = __ballot_sync(0xffffffffu, e < E) & ~m0[k];
         if (e < E) {
           const int dst = ((m0[k] >> lane) & 1u) ? r0 + __popc(m0[k] & lt) : n0 + r1 + __popc(ones & lt);
-          sK[dst] = zk[k];
+          sZ[dst] = zk[k];  // in place: every thread read its keys before the barrier above
           sIdx[dst] = (uint16_t)e;
         }
         r0 += __popc(m0[k]);
@@ -502,8 +505,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
       }
       __syncthreads();
       const int n1 = E - n0;
-      const uint64_t* K0 = sK;
-      const uint64_t* K1 = sK + n0;
+      const uint64_t* K0 = sZ;
+      const uint64_t* K1 = sZ + n0;
       const int d = base_e < E ? base_e : E;
       int lo = d - n1 > 0 ? d - n1 : 0, hi = d < n0 ? d : n0;
       while (lo < hi) {
@@ -537,7 +540,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
       for (int k = 0; k < kPerThread; ++k) {
         if (d + k < E) {
           sZ[d + k] = rz[k];
-          sPerm[d + k] = rp[k];  // the amplitudes stay where they were loaded
+          sPerm[d + k] = rp[k];  // the amplitudes stay where they were loaded (sIdx was read above)
         }
       }
       __syncthreads();
@@ -581,8 +584,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_tile(OpArgs a) {
       constexpr int MC = KindTraits<KIND>::kMaxChildren;
       uint64_t kb;
       double2 ca[MC];
-      uint16_t* sOff = sIdx;                              // free after the merge
-      uint8_t* sMask = reinterpret_cast<uint8_t*>(sK) + 2 * kTilePad;  // after sPerm
+
       const int wmode = a.write_mode;
       // (a) kept-children mask per position
       for (int p = tid; p < E; p += kThreads) {
@@ -1685,7 +1687,7 @@ __global__ void k_rdm_final(const bass_state* st, double* rho, WsView ws, int fi
 // ---------------------------------------------------------------------------
 template <int KIND, int PASS>
 static cudaError_t launch_tile(OpArgs a, int counter, cudaStream_t s, int* grid_out) {
-  const size_t smem = (size_t)kTilePad * (16 + 8 + 8 + 2);
+  const size_t smem = (size_t)kTilePad * (16 + 8 + 2 + (PASS == P_WRITE ? 3 : 0));
   static int grid = 0;
   if (grid == 0) {
     cudaError_t e = cudaFuncSetAttribute(k_tile<KIND, PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
