@@ -172,6 +172,18 @@ struct KindTraits {
 // start a group); child o has the new physical key base | o and amplitude
 // ca[o].  Within a group, entries are in ascending local index, so the sums
 // run over the local index in ascending order.
+// The rotation's drop rule hypot(re, im) > 1e-30 (bass_simulator.py:156-199),
+// decided without calling hypot outside a narrow band: hypot lies between
+// max(|re|, |im|) and sqrt(2) max(|re|, |im|) (within its last-place error),
+// so the answer is known unless max is within [7e-31, 1e-30].
+__device__ __forceinline__ bool above_drop(double2 c) {
+  if (c.x != c.x || c.y != c.y) return hypot(c.x, c.y) > 1e-30;  // NaN: as hypot decides
+  const double m = fmax(fabs(c.x), fabs(c.y));
+  if (m > 1e-30) return true;
+  if (m < 7e-31) return false;
+  return hypot(c.x, c.y) > 1e-30;
+}
+
 // The tile's amplitudes as the evaluation sees them: stored in load order,
 // read at Z position p through the merge's permutation (identity when there
 // is none), with the state's pending renormalisation applied.
@@ -237,7 +249,7 @@ __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t*
     for (int o = 0; o < 2; ++o) {
       const double2 c = cadd(cmul(sG[o * 2], a0), cmul(sG[o * 2 + 1], a1));
       ca[o] = c;
-      if (hypot(c.x, c.y) > 1e-30) mask |= 1u << o;
+      if (above_drop(c)) mask |= 1u << o;
     }
   }
   return mask;
