@@ -262,6 +262,7 @@ def run_ours(a, rank, world, dist):
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
             "amp_updates_per_step": int(statistics.mean(ups)), "kernels": kernels,
+            "bass_stats": {k: int(v) for k, v in b.stats.items()},
         }
         print(json.dumps(line), flush=True)
 
