@@ -310,6 +310,7 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
     step_bytes = 24 * (sum(int(c["prof_in"][k * 5 + 0]) for k in kinds) +
                        sum(int(c["prof_out"][k * 5 + 3]) for k in kinds))
     step_gbs = step_bytes / (step_ms * 1e-3) / 1e9
+    top = int(np.argmax(ms))  # the longest kernel overall (the selection has no algorithmic bytes of its own)
     roof = {"bound": "hbm", "kernel": nat.SLOT_NAMES[dom], "achieved": round(achieved, 1), "peak": peak,
             "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "bytes_per_launch": per_launch_bytes,
@@ -317,6 +318,9 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
                            "bytes_per_step": step_bytes,
                            "note": "24 B per entry read + 24 B per entry written by every gate, rotation step "
                                    "and truncation, over the timed step"},
+            "longest_kernel": {"kernel": nat.SLOT_NAMES[top], "share": round(float(ms[top] / ms.sum()), 4),
+                               "note": "radix select over the slot array: overhead traffic only, so the "
+                                       "roofline above is that of the longest kernel with algorithmic bytes"},
             "note": "algorithmic bytes = 24 B per entry read + 24 B per entry written; timing from a "
                     "profiled step (CUDA events around each launch on its stream)"}
     return roof, kernels[:12]
