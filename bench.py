@@ -319,8 +319,8 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
                            "note": "24 B per entry read + 24 B per entry written by every gate, rotation step "
                                    "and truncation, over the timed step"},
             "longest_kernel": {"kernel": nat.SLOT_NAMES[top], "share": round(float(ms[top] / ms.sum()), 4),
-                               "note": "radix select over the slot array: overhead traffic only, so the "
-                                       "roofline above is that of the longest kernel with algorithmic bytes"},
+                               "note": "share of the profiled step; the roofline above is that of the "
+                                       "longest tile pass, the kernels that move the state's own bytes"},
             "note": "algorithmic bytes = 24 B per entry read + 24 B per entry written; timing from a "
                     "profiled step (CUDA events around each launch on its stream)"}
     return roof, kernels[:12]
