@@ -368,33 +368,6 @@ __device__ __forceinline__ void hist_add(unsigned int* h, unsigned bin, bool val
   if (valid && (__ffs(peers) - 1) == lane) atomicAdd(&h[bin], (unsigned)__popc(peers));
 }
 
-// Calls f(bits, index) for every slot of slots[0, nslots), four 16-byte loads
-// in flight per thread.  Loop bounds are uniform per warp and every lane
-// calls f the same number of times (out-of-range lanes get bits = ~0), so f
-// may use warp-synchronous primitives.
-template <class F>
-__device__ __forceinline__ void scan_slots(const unsigned long long* slots, long long nslots, F&& f) {
-  const ulonglong2* v = reinterpret_cast<const ulonglong2*>(slots);
-  const long long n2 = nslots >> 1;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long b = (long long)blockIdx.x * blockDim.x; b < n2; b += 4 * stride) {
-    ulonglong2 x[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const long long i = b + u * stride + threadIdx.x;
-      x[u] = (i < n2) ? v[i] : make_ulonglong2(~0ULL, ~0ULL);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const long long i = b + u * stride + threadIdx.x;
-      f(x[u].x, 2 * i);
-      f(x[u].y, 2 * i + 1);
-    }
-  }
-  if ((nslots & 1) && blockIdx.x == 0 && threadIdx.x < 32)
-    f(threadIdx.x == 0 ? slots[nslots - 1] : ~0ULL, nslots - 1);
-}
-
 // ---------------------------------------------------------------------------
 // workspace
 // ---------------------------------------------------------------------------
@@ -411,15 +384,11 @@ struct Partial {
 struct SelState {
   long long n_out;       // children produced by the op (after drop rules)
   long long k_keep;
-  long long need;        // entries still to take from the boundary bin
-  long long n_cand;
-  unsigned long long prefix;
+  long long n_cand;      // children of the level-2 boundary bin collected by the count pass
   unsigned long long t_bits;
-  unsigned long long t_key;
+  unsigned long long t_key;  // ~0: every child at t_bits kept; else the largest kept true key there
   int do_trunc;
-  int stage;             // 0 keep all, 1 level-1 bin known, 2 level-2 bin known, 3 resolved,
-                         // 4 exact tie at bits == prefix: settle by true key
-  int cand_overflow;
+  int stage;             // 0 keep all, 3 threshold resolved
   int pad;               // K_IDENT guard: a zero amplitude was produced
   double total;          // exact sum of |a|^2 over the op's output (truncating ops only)
   long long n_written;
@@ -428,9 +397,7 @@ struct SelState {
   int skip_write;        // the write pass has nothing to do (rejected rotation)
   int accept;            // rotation step: the candidate lowers PR
   double pr_new;         // rotation step: PR of the candidate
-  int tie;               // the threshold was settled by key (stage 4 was taken)
-  int tie_overflow;      // the tied children did not fit the candidate arrays
-  long long n_tie;       // tied children collected by the P_GATHER pass
+  int8_t qat[64];        // output qubit order, for the key tie-break at t_bits
 };
 
 struct WsView {

@@ -44,12 +44,20 @@ struct Hdr {
   int8_t qat_out[64];
 };
 
-__device__ __forceinline__ void out_order(const bass_state* in, int kind, int t, int gb, int8_t* qat_out) {
-  for (int p = 0; p < 64; ++p) qat_out[p] = in->qat[p];
-  if (kind == K_GATE1 || kind == K_ROT1 || kind == K_GATE2 || kind == K_PERM) {
-    int8_t qt = in->qat[t];
-    for (int p = t; p > gb; --p) qat_out[p] = in->qat[p - 1];
-    qat_out[gb] = qt;
+// The op's output qubit order: the input's, with the target qubit's
+// position t = pos[q] moved down to gb (positions gb..t-1 move up by one) for
+// the kinds that bring a target to the low bits.  One position per thread
+// (threads 0-63 of the block); the caller synchronises before reading it.
+__device__ __forceinline__ void out_order_par(const bass_state* in, int kind, int q, int gb, int8_t* qat_out) {
+  const int p = threadIdx.x;
+  if (p < 64) {
+    int src = p;
+    if (kind == K_GATE1 || kind == K_ROT1 || kind == K_GATE2 || kind == K_PERM) {
+      const int t = in->pos[q];
+      if (p > gb && p <= t) src = p - 1;
+      if (p == gb) src = t;
+    }
+    qat_out[p] = in->qat[src];
   }
 }
 
@@ -263,13 +271,10 @@ __device__ __forceinline__ bool keep_child(uint64_t bits, uint64_t key, const Se
   return S.t_key == ~0ULL || true_key(key, qat, 64) <= S.t_key;
 }
 
-// Slot value of a child at the threshold that survives the key tie-break:
-// above every probability's bit pattern (a NaN payload) and distinct from ~0.
-constexpr unsigned long long kSlotKeptTie = 0x7FFFFFFFFFFFFFFEULL;
-
 // Does the child with this slot survive the selection?  (T, incl) = (t_bits,
-// t_key == ~0) when truncating, (0, true) otherwise; ties settled by key were
-// rewritten to kSlotKeptTie / 0 by the selection.
+// t_key == ~0) when truncating, (0, true) otherwise.  With incl false the
+// children at exactly T are settled by true key (keep_child, and k_compact's
+// check against t_key).
 __device__ __forceinline__ bool slot_kept(unsigned long long bits, unsigned long long T, bool incl) {
   return bits != ~0ULL && (bits > T || (incl && bits == T));
 }
@@ -288,6 +293,7 @@ __host__ __device__ constexpr int slots_per_entry(int kind) {
 // One thread.  Runs in the last CTA of the write pass to finish, so the
 // selection's results (written by the previous kernel) and n_written (written
 // by the CTA of the last tile, before its fence) are read through volatile.
+// The output's qubit order is written by write_done.
 __device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int kind) {
   volatile SelState* sel = a.ws.sel;
   const bass_state* in = a.in;
@@ -299,13 +305,6 @@ __device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int
   if (nw > out->cap) {  // the write pass skipped the tiles that did not fit
     set_error(c, BASS_ERR_CAPACITY);
     nw = 0;
-  }
-  const int t = (kind == K_IDENT) ? 0 : in->pos[a.q];
-  int8_t qat[64];
-  out_order(in, kind, t, a.gb, qat);
-  for (int p = 0; p < 64; ++p) {
-    out->qat[p] = qat[p];
-    out->pos[qat[p]] = (int8_t)p;
   }
   out->nq = in->nq;
   out->nnz = nw;
@@ -338,6 +337,30 @@ __device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int
   if (tr.mark_active) {
     c->truncation_active = 1;
     c->gates_since_trunc = 0;
+  }
+}
+
+// Block-wide, at the end of a write pass: the last CTA to arrive writes the
+// output descriptor (its qubit order one position per thread, the rest by
+// finalize_op).
+__device__ void write_done(const OpArgs& a, int kind) {
+  __shared__ int sLastW;
+  __shared__ int8_t sQo[64];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned long long d = atomicAdd(&reinterpret_cast<unsigned long long*>(a.ws.counters)[59], 1ULL);
+    sLastW = (d == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!sLastW) return;
+  __threadfence();
+  out_order_par(a.in, kind, a.q, a.gb, sQo);
+  __syncthreads();
+  if (threadIdx.x == 0) finalize_op(a, a.tr, a.fin_mode, kind);
+  if (threadIdx.x < 64) {
+    a.out->qat[threadIdx.x] = sQo[threadIdx.x];
+    a.out->pos[sQo[threadIdx.x]] = (int8_t)threadIdx.x;
   }
 }
 
@@ -385,8 +408,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
     H.nq = in->nq;
     H.t = (KIND == K_IDENT || KIND == K_RDM) ? 0 : in->pos[a.q];
     H.ntiles = (KIND == K_IDENT) ? plain_tiles(H.n) : merge_tiles(H.n);
-    out_order(in, KIND, H.t, a.gb, H.qat_out);
   }
+  out_order_par(a.in, KIND, a.q, a.gb, H.qat_out);
   __syncthreads();
 
   const int gb = a.gb;
@@ -710,18 +733,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
   }
 
   // ---- write pass: the last CTA to finish writes the output descriptor ------
-  if (PASS == P_WRITE && a.fin) {
-    __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      const unsigned long long d =
-          atomicAdd(&reinterpret_cast<unsigned long long*>(a.ws.counters)[59], 1ULL);
-      if (d == gridDim.x - 1) {
-        __threadfence();
-        finalize_op(a, a.tr, a.fin_mode, KIND);
-      }
-    }
-  }
+  if (PASS == P_WRITE && a.fin) write_done(a, KIND);
 
   // ---- flush: the CTA's child count ----------------------------------------
   if (PASS == P_HIST) {
@@ -746,18 +758,22 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
 //   1. the child count (from the evaluation pass's per-CTA partials) decides
 //      whether the op truncates;
 //   2. radix select on the bit patterns: a 13-bit histogram of bits 50-62,
-//      then of bits 37-49 inside the boundary bin, then the exact candidates
-//      of the boundary bin (block 0); every block reads the histograms and
-//      finds the boundary bins itself, so each level costs one grid barrier;
+//      then of bits 37-49 inside the boundary bin; every block reads the
+//      histograms and finds the boundary bins itself, so each level costs
+//      one grid barrier;
 //   3. per tile, the number of survivors (into ws.status) and per CTA the
-//      exact kept mass, total mass and, for a rotation step, sum of |a|^4;
+//      exact kept mass, total mass and, for a rotation step, sum of |a|^4.
+//      When the threshold lies inside the level-2 bin, this pass keeps what
+//      lies above the bin and collects the bin's children (slot, true key);
+//      after a barrier every block settles them (the k-th best by bits, then
+//      smallest true key: settle_small, or settle_radix in block 0 for more
+//      than kCandSmem) and adds the kept ones to the tile counts and sums;
 //   4. the last block to finish step 3: the exact sums, the rotation
 //      decision, and an exclusive scan of the tile counts (each tile of the
 //      write step then knows its base).
-// An exact tie at the threshold (equal bit patterns straddling rank k) is
-// settled inside step 2: the tied children's true keys are read from the
-// staged keys, the smallest `need` of them survive, and their slots are
-// rewritten as kept / dropped before step 3.  The grid barrier is a counter and a generation word in the
+// Children tied at the threshold pattern t_bits are kept up to the largest
+// kept true key t_key; the write step applies the same rule.  The grid
+// barrier is a counter and a generation word in the
 // workspace with a bounded spin (BASS_ERR_WAIT, then every block returns).
 constexpr int kSelThreads = 512;
 
@@ -917,22 +933,15 @@ __device__ __forceinline__ bool better(unsigned long long ab, unsigned long long
   return ab > bb || (ab == bb && ak < bk);
 }
 
-// Sorts the first m candidates by (bits desc, key asc) in shared memory
-// (m <= kCandSmem).  by_key_only: the candidates all share one bit pattern
-// and cand_bits holds their slot indices.
-__device__ void sort_candidates(unsigned long long* sb, unsigned long long* sk, long long m, const WsView& ws,
-                                bool by_key_only) {
+// Sorts sb / sk [0, m) (m <= kCandSmem) by (bits desc, key asc): bitonic,
+// padded to a power of two with pairs that rank below every candidate.
+__device__ void sort_pairs(unsigned long long* sb, unsigned long long* sk, long long m) {
   const int tid = threadIdx.x;
   int P = 1;
   while (P < m) P <<= 1;
-  for (int i = tid; i < P; i += blockDim.x) {
-    if (i < m) {
-      sb[i] = by_key_only ? 1ULL : __ldcg(ws.cand_bits + i);
-      sk[i] = __ldcg(ws.cand_key + i);
-    } else {
-      sb[i] = 0;
-      sk[i] = ~0ULL;
-    }
+  for (int i = tid + (int)m; i < P; i += blockDim.x) {
+    sb[i] = 0;
+    sk[i] = ~0ULL;
   }
   __syncthreads();
   for (int size = 2; size <= P; size <<= 1) {
@@ -953,220 +962,116 @@ __device__ void sort_candidates(unsigned long long* sb, unsigned long long* sk, 
   }
 }
 
-// Result of exact_select (in shared memory of the calling block).
-struct ExactOut {
-  int stage;                 // 3 resolved, 4 exact tie to settle by key
-  unsigned long long t_bits; // stage 3: the threshold bit pattern
-  unsigned long long t_key;  // stage 3: ~0 (every child at t_bits kept) or the largest kept key
-  unsigned long long prefix; // stage 4: the tied bit pattern
-  long long need;            // stage 4: tied children to keep
-};
-
-// One block.  mode 0: the m candidates (bits, slot) of the level-2 boundary
-//   bin (pre, need: its 26-bit prefix and the survivors still to take from
-//   it); find the need-th largest bit pattern T.  If every candidate equal to
-//   T is needed the threshold is resolved (keep bits >= T, stage 3);
-//   otherwise the tie is settled by true key (stage 4: the tied children are
-//   collected with their keys).  Several blocks may run it on the same
-//   candidates; only the one with writer set writes the selection state.
-// mode 1 (stage 4, one block): the candidates are (slot, true key) of the
-//   children at T; keep the need smallest keys (stage 3 with t_key).
-__device__ void exact_select(const OpArgs& a, int mode, unsigned char* smem, long long m_in, bool overflow,
-                             long long need_in, unsigned long long pre_in, bool writer, ExactOut* out) {
+// The threshold of the level-2 boundary bin's m candidates (slot index in
+// ws.cand_bits, true key in ws.cand_key; m <= kCandSmem), one block: the
+// need-th best child by (bits desc, key asc) gives (t_bits, t_key); t_key is
+// ~0 when every candidate at t_bits is kept.  Every block of the selection
+// runs it on the same candidates and reaches the same pair.
+__device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, long long need,
+                             unsigned long long* tb_out, unsigned long long* tk_out) {
   unsigned long long* sb = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* sk = sb + kCandSmem;
-  SelState* sel = a.ws.sel;
-  __shared__ long long sM, sNeedIn;
-  __shared__ unsigned long long sPre;
-  if (threadIdx.x == 0) {
-    long long m = m_in;
-    if (overflow || m > a.ws.max_n) {
-      if (writer) set_error(a.ctrl, BASS_ERR_WORKSPACE);
-      m = a.ws.max_n;
-    }
-    sM = m;
-    sNeedIn = need_in;
-    sPre = pre_in;
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  const int tid = threadIdx.x;
+  for (long long i = tid; i < m; i += blockDim.x) {
+    sb[i] = __ldcg(slots + __ldcg(a.ws.cand_bits + i));
+    sk[i] = __ldcg(a.ws.cand_key + i);
   }
   __syncthreads();
-  const long long m = sM, need = sNeedIn;
-  const int tid = threadIdx.x;
-  __shared__ unsigned long long sT;
-  __shared__ long long sGt, sEq;
+  const long long r = need < 1 ? 0 : (need > m ? m - 1 : need - 1);
+  __shared__ int sSel, sCut;
+  if (tid == 0) { sSel = 0; sCut = 0; }
+  __syncthreads();
   if (m <= kRankMax) {
-    // few candidates: the rank of each is the number that rank above it
-    for (long long i = tid; i < m; i += blockDim.x) {
-      sb[i] = (mode == 1) ? 1ULL : __ldcg(a.ws.cand_bits + i);
-      sk[i] = __ldcg(a.ws.cand_key + i);
-    }
-    __shared__ int sSel, sGtI, sEqI;
-    if (tid == 0) { sSel = 0; sGtI = 0; sEqI = 0; }
-    __syncthreads();
-    const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
+    // few: the rank of each candidate is the number that rank above it
     for (long long i = tid; i < m; i += blockDim.x) {
       long long rank = 0;
       for (long long jx = 0; jx < m; ++jx) rank += better(sb[jx], sk[jx], sb[i], sk[i]);
       if (rank == r) sSel = (int)i;
     }
-    __syncthreads();
-    const unsigned long long Tsel = sb[sSel];
-    if (mode == 0) {
-      for (long long i = tid; i < m; i += blockDim.x) {
-        if (sb[i] > Tsel) atomicAdd(&sGtI, 1);
-        else if (sb[i] == Tsel) atomicAdd(&sEqI, 1);
-      }
-    }
-    __syncthreads();
-    if (tid == 0) {
-      if (mode == 1) {
-        out->stage = 3;
-        out->t_bits = sPre;
-        out->t_key = sk[sSel];
-        if (writer) {
-          sel->t_bits = sPre;
-          sel->t_key = sk[sSel];
-          sel->stage = 3;
-        }
-      } else {
-        sT = Tsel;
-        sGt = sGtI;
-        sEq = sEqI;
-      }
-    }
-    if (mode == 1) {
-      __syncthreads();
-      return;
-    }
-  } else if (m <= kCandSmem) {
-    sort_candidates(sb, sk, m, a.ws, mode == 1);
-    const long long r = (need >= 1 && need <= m) ? need - 1 : 0;
-    if (mode == 1) {
-      if (tid == 0) {
-        out->stage = 3;
-        out->t_bits = sPre;
-        out->t_key = sk[r];
-        if (writer) {
-          sel->t_bits = sPre;
-          sel->t_key = sk[r];
-          sel->stage = 3;
-        }
-      }
-    } else {
-      // sorted descending: the entries above T precede the run equal to T
-      const unsigned long long T = sb[r];
-      __shared__ int sLo, sHi;
-      if (tid == 0) { sLo = (int)r; sHi = (int)r; }
-      __syncthreads();
-      for (long long i = tid; i < m; i += blockDim.x) {
-        if (sb[i] == T) {
-          atomicMin(&sLo, (int)i);
-          atomicMax(&sHi, (int)i);
-        }
-      }
-      __syncthreads();
-      if (tid == 0) { sT = T; sGt = sLo; sEq = sHi - sLo + 1; }
-    }
-  } else if (mode == 1) {
-    // all candidates share the bit pattern: radix select of the need-th smallest key
-    unsigned int* h = reinterpret_cast<unsigned int*>(smem);
-    __shared__ unsigned long long sKeyPre;
-    __shared__ long long sNeed;
-    if (tid == 0) { sKeyPre = 0; sNeed = need; }
-    __syncthreads();
-    for (int shift = 56; shift >= 0; shift -= 8) {
-      for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
-      __syncthreads();
-      const unsigned long long pre = sKeyPre;
-      for (long long i = tid; i < m; i += blockDim.x) {
-        const unsigned long long k = __ldcg(a.ws.cand_key + i);
-        if (shift == 56 || (k >> (shift + 8)) == pre) atomicAdd(&h[(unsigned)(k >> shift) & 255u], 1u);
-      }
-      __syncthreads();
-      if (tid == 0) {
-        long long below = 0;
-        int b = 0;
-        for (; b < 255; ++b) {
-          if (below + h[b] >= sNeed) break;
-          below += h[b];
-        }
-        sNeed -= below;
-        sKeyPre = (pre << 8) | (unsigned long long)b;
-      }
-      __syncthreads();
-    }
-    if (tid == 0) {
-      out->stage = 3;
-      out->t_bits = sPre;
-      out->t_key = sKeyPre;
-      if (writer) {
-        sel->t_bits = sPre;
-        sel->t_key = sKeyPre;
-        sel->stage = 3;
-      }
-    }
-    __syncthreads();
-    return;
   } else {
-    // many candidates: radix select on the low 37 bits of the bit pattern
-    unsigned int* h = reinterpret_cast<unsigned int*>(smem);
-    __shared__ unsigned long long sLow;
-    __shared__ long long sNeed;
-    __shared__ unsigned int sLastCount;
-    if (tid == 0) { sLow = 0; sNeed = need; }
-    __syncthreads();
-    const unsigned long long m37 = (1ULL << 37) - 1;
-    for (int shift = 32; shift >= 0; shift -= 8) {
-      for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
-      __syncthreads();
-      const unsigned long long pre = sLow;
-      for (long long i = tid; i < m; i += blockDim.x) {
-        const unsigned long long lb = __ldcg(a.ws.cand_bits + i) & m37;
-        if (shift == 32 || (lb >> (shift + 8)) == pre) atomicAdd(&h[(unsigned)(lb >> shift) & 255u], 1u);
-      }
-      __syncthreads();
-      if (tid == 0) {
-        long long above = 0;
-        int b = 255;
-        for (; b > 0; --b) {
-          if (above + h[b] >= sNeed) break;
-          above += h[b];
-        }
-        sNeed -= above;
-        sLow = (pre << 8) | (unsigned long long)b;
-        sLastCount = h[b];
-      }
-      __syncthreads();
-    }
-    if (tid == 0) {
-      sT = (sPre << 37) | sLow;
-      sGt = need - sNeed;
-      sEq = sLastCount;
-    }
+    sort_pairs(sb, sk, m);
+    if (tid == 0) sSel = (int)r;
   }
   __syncthreads();
-  if (tid == 0 && mode == 0) {
-    const long long take = need - sGt;  // entries equal to T that are kept
-    if (take == sEq) {
-      out->stage = 3;
-      out->t_bits = sT;
-      out->t_key = ~0ULL;
-      if (writer) {
-        sel->t_bits = sT;
-        sel->t_key = ~0ULL;
-        sel->stage = 3;
-      }
-    } else {
-      out->stage = 4;
-      out->prefix = sT;
-      out->need = take;
-      if (writer) {
-        sel->stage = 4;
-        sel->tie = 1;
-        sel->prefix = sT;
-        sel->need = take;
-      }
+  const unsigned long long tb = sb[sSel], tk = sk[sSel];
+  for (long long i = tid; i < m; i += blockDim.x)
+    if (sb[i] == tb && sk[i] > tk) sCut = 1;
+  __syncthreads();
+  *tb_out = tb;
+  *tk_out = sCut ? tk : ~0ULL;
+  __syncthreads();  // smem is reused by the caller
+}
+
+// The same threshold for m > kCandSmem (block 0 alone): radix select on the
+// low 37 bits of the bit pattern (the 26-bit prefix pre is shared), then, if
+// the cut falls inside a run of equal patterns, on the true keys of that run.
+__device__ void settle_radix(const OpArgs& a, unsigned char* smem, long long m, long long need,
+                             unsigned long long pre, unsigned long long* tb_out, unsigned long long* tk_out) {
+  unsigned int* h = reinterpret_cast<unsigned int*>(smem);
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  const int tid = threadIdx.x;
+  __shared__ unsigned long long sLow, sKeyPre;
+  __shared__ long long sNeed;
+  __shared__ unsigned int sLastCount;
+  if (tid == 0) { sLow = 0; sNeed = need; sKeyPre = 0; }
+  __syncthreads();
+  const unsigned long long m37 = (1ULL << 37) - 1;
+  for (int shift = 32; shift >= 0; shift -= 8) {
+    for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const unsigned long long p = sLow;
+    for (long long i = tid; i < m; i += blockDim.x) {
+      const unsigned long long lb = __ldcg(slots + __ldcg(a.ws.cand_bits + i)) & m37;
+      if (shift == 32 || (lb >> (shift + 8)) == p) atomicAdd(&h[(unsigned)(lb >> shift) & 255u], 1u);
     }
+    __syncthreads();
+    if (tid == 0) {
+      long long above = 0;
+      int b = 255;
+      for (; b > 0; --b) {
+        if (above + h[b] >= sNeed) break;
+        above += h[b];
+      }
+      sNeed -= above;
+      sLow = (p << 8) | (unsigned long long)b;
+      sLastCount = h[b];
+    }
+    __syncthreads();
   }
+  const unsigned long long tb = (pre << 37) | sLow;
+  const long long take = sNeed;  // children at tb that are kept
+  if (take >= (long long)sLastCount) {
+    *tb_out = tb;
+    *tk_out = ~0ULL;
+    __syncthreads();
+    return;
+  }
+  // the take smallest true keys among the children at tb
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const unsigned long long p = sKeyPre;
+    for (long long i = tid; i < m; i += blockDim.x) {
+      if (__ldcg(slots + __ldcg(a.ws.cand_bits + i)) != tb) continue;
+      const unsigned long long k = __ldcg(a.ws.cand_key + i);
+      if (shift == 56 || (k >> (shift + 8)) == p) atomicAdd(&h[(unsigned)(k >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      long long below = 0;
+      int b = 0;
+      for (; b < 255; ++b) {
+        if (below + h[b] >= sNeed) break;
+        below += h[b];
+      }
+      sNeed -= below;
+      sKeyPre = (p << 8) | (unsigned long long)b;
+    }
+    __syncthreads();
+  }
+  *tb_out = tb;
+  *tk_out = sKeyPre;
   __syncthreads();
 }
 
@@ -1186,12 +1091,11 @@ __device__ __forceinline__ long long tile_of(long long z, int kind, const long l
 // which the op cleared; one atomic per warp when its 256 slots lie in one
 // tile) and, per CTA in partials s[0..2], the exact mass of the survivors,
 // their sum of |a|^4 (P2) and the exact mass of all children (when
-// truncating).  Slots rewritten by a key tie-break (kSlotKeptTie, 0) carry
-// no mass here; final_phase adds the tied children back.
+// truncating).  cand: the children of the level-2 boundary bin (bits >> 37 ==
+// cpre, all below T) are collected for settle_small / settle_radix as well.
 template <bool P2>
 __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long long T, bool incl, bool trunc,
-                            i128* sRed, int* sCnt) {
-  (void)sCnt;
+                            i128* sRed, bool cand, unsigned long long cpre, const int8_t* qat) {
   const long long n = a.in->nnz;
   const long long nslots = (long long)ns * n;
   const bool sums = P2 || trunc;
@@ -1219,12 +1123,41 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
 #pragma unroll
       for (int u = 0; u < 8; ++u) x[u] = (s0 + u < nslots) ? slots[s0 + u] : ~0ULL;
     }
+    if (cand) {
+      // the boundary bin's children: appended (slot, true key) to the
+      // candidate arrays, one atomic per warp
+      unsigned cm = 0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) cm |= (unsigned)(x[u] != ~0ULL && (x[u] >> 37) == cpre) << u;
+      if (__any_sync(0xffffffffu, cm != 0)) {
+        const int cc = __popc(cm);
+        int inc = cc;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, inc, off);
+          if (lane >= off) inc += y;
+        }
+        unsigned long long base = 0;
+        if (lane == 31)
+          base = atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws.sel->n_cand), (unsigned long long)inc);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        long long k = (long long)base + inc - cc;
+        for (int u = 0; u < 8; ++u) {
+          if (!((cm >> u) & 1u)) continue;
+          if (k < a.ws.max_n) {
+            a.ws.cand_bits[k] = (unsigned long long)(s0 + u);
+            a.ws.cand_key[k] = true_key(a.ws.stage_keys[s0 + u], qat, 64);
+          }
+          ++k;
+        }
+      }
+    }
     unsigned km = 0;
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const bool kept = slot_kept(x[u], T, incl);
       km |= (unsigned)kept << u;
-      if (sums && x[u] != ~0ULL && x[u] != kSlotKeptTie) {
+      if (sums && x[u] != ~0ULL) {
         const i128 f = fx_from_pbits(x[u]);
         if (want_total) v[2] += f;
         if (kept) {
@@ -1285,13 +1218,6 @@ __device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j
   block_sum_i128<3>(v, sRed);
   if (threadIdx.x == 0) {
     const int trunc = sel->do_trunc;
-    if (trunc && sel->tie) {  // the tied children's slots were rewritten: add them back
-      const double T = __longlong_as_double((long long)sel->t_bits);
-      const i128 f = fx_from(T);
-      v[0] += (i128)sel->need * f;
-      v[1] += (i128)sel->need * fx_from(__dmul_rn(T, T));
-      v[2] += (i128)sel->n_tie * f;
-    }
     const double kept = fx_to(v[0]);
     const double p2 = fx_to(v[1]);
     sel->kept = kept;
@@ -1374,7 +1300,6 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
   unsigned int* h = reinterpret_cast<unsigned int*>(smem);
   __shared__ long long sS[kSelThreads / 32];
   __shared__ i128 sRed[3 * (kSelThreads / 32)];
-  __shared__ int sCnt[kSelThreads / 32];
   __shared__ long long sNout;
   SelState* sel = a.ws.sel;
   const int tid = threadIdx.x;
@@ -1403,6 +1328,9 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
   const bool trunc = !(a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out);
   unsigned long long T = 0ULL, tkey = ~0ULL;
   bool incl = true;
+  bool late = false;  // the threshold lies inside the level-2 bin lpre
+  unsigned long long lpre = 0;
+  long long lneed = 0;
   if (trunc && a.k_keep <= 0) {
     T = ~0ULL;
     tkey = 0ULL;
@@ -1426,106 +1354,12 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
       if (c_b2 == need2) {
         T = pre << 37;
       } else {
-        scan_slots(slots, nslots, [&](unsigned long long bits, long long i) {
-          if (bits != ~0ULL && (bits >> 37) == pre) {
-            const unsigned long long k = atomicAdd(reinterpret_cast<unsigned long long*>(&sel->n_cand), 1ULL);
-            if ((long long)k < a.ws.max_n) {
-              a.ws.cand_bits[k] = bits;
-              a.ws.cand_key[k] = (unsigned long long)i;
-            } else {
-              sel->cand_overflow = 1;
-            }
-          }
-        });
-        if (blockIdx.x == 0 && tid == 0) {
-          sel->prefix = pre;
-          sel->need = need2;
-          sel->stage = 2;
-          sel->do_trunc = 1;
-          sel->n_out = n_out;
-          sel->k_keep = a.k_keep;
-        }
-        if (!grid_sync(a)) return;
-        // few candidates (the usual case): every block settles them itself,
-        // block 0 records the result; many: block 0 alone, then a barrier
-        __shared__ ExactOut eo;
-        __shared__ long long sMc;
-        __shared__ int sOvf;
-        if (tid == 0) {
-          sMc = *(volatile long long*)&sel->n_cand;
-          sOvf = *(volatile int*)&sel->cand_overflow;
-        }
-        __syncthreads();
-        const long long mc = sMc;
-        if (mc <= kCandSmem && !sOvf) {
-          exact_select(a, 0, smem, mc, false, need2, pre, blockIdx.x == 0, &eo);
-        } else {
-          if (blockIdx.x == 0) exact_select(a, 0, smem, mc, sOvf != 0, need2, pre, true, &eo);
-          if (!grid_sync(a)) return;
-          if (tid == 0) {  // block 0's result, for every block
-            volatile SelState* vs = sel;
-            eo.stage = vs->stage;
-            eo.t_bits = vs->t_bits;
-            eo.prefix = vs->prefix;
-            eo.need = vs->need;
-          }
-          __syncthreads();
-        }
-        if (eo.stage != 4) {
-          T = eo.t_bits;
-        } else {
-          // An exact tie at T: the survivors among the children at T are the
-          // `need` smallest true keys.  Their keys come from the staging
-          // array (new physical keys, mapped back through the output order).
-          if (!grid_sync(a)) return;  // every block is done with the level-2 candidates
-          __shared__ int8_t sQat[64];
-          if (tid == 0) out_order(a.in, kind, kind == K_IDENT ? 0 : a.in->pos[a.q], a.gb, sQat);
-          __syncthreads();
-          const unsigned long long Tt = eo.prefix;
-          scan_slots(slots, nslots, [&](unsigned long long bits, long long i) {
-            if (bits == Tt) {
-              const unsigned long long k =
-                  atomicAdd(reinterpret_cast<unsigned long long*>(&sel->n_tie), 1ULL);
-              if ((long long)k < a.ws.max_n) {
-                a.ws.cand_bits[k] = (unsigned long long)i;
-                a.ws.cand_key[k] = true_key(a.ws.stage_keys[i], sQat, 64);
-              } else {
-                sel->tie_overflow = 1;
-              }
-            }
-          });
-          if (!grid_sync(a)) return;
-          __shared__ ExactOut eo2;
-          __shared__ long long sMt;
-          __shared__ int sOvt;
-          if (tid == 0) {
-            sMt = *(volatile long long*)&sel->n_tie;
-            sOvt = *(volatile int*)&sel->tie_overflow;
-          }
-          __syncthreads();
-          const long long mt = sMt;
-          if (mt <= kCandSmem && !sOvt) {
-            exact_select(a, 1, smem, mt, false, eo.need, Tt, blockIdx.x == 0, &eo2);
-          } else {
-            if (blockIdx.x == 0) exact_select(a, 1, smem, mt, sOvt != 0, eo.need, Tt, true, &eo2);
-            if (!grid_sync(a)) return;
-            if (tid == 0) eo2.t_key = *(volatile unsigned long long*)&sel->t_key;
-            __syncthreads();
-          }
-          T = Tt;
-          tkey = eo2.t_key;
-          incl = false;
-          // rewrite the tied slots as kept / dropped, so that the survivors
-          // are decided by the slot alone from here on
-          unsigned long long* wslots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys);
-          const long long mm = mt < a.ws.max_n ? mt : a.ws.max_n;
-          for (long long k = (long long)blockIdx.x * blockDim.x + tid; k < mm;
-               k += (long long)gridDim.x * blockDim.x) {
-            const unsigned long long i = __ldcg(a.ws.cand_bits + k);
-            if ((long long)i < nslots) wslots[i] = (__ldcg(a.ws.cand_key + k) <= tkey) ? kSlotKeptTie : 0ULL;
-          }
-          if (!grid_sync(a)) return;
-        }
+        // the bin's children are settled after the count pass, which keeps
+        // everything above the bin and collects the bin itself
+        late = true;
+        lpre = pre;
+        lneed = need2;
+        T = (pre + 1) << 37;
       }
     }
   }
@@ -1537,8 +1371,73 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
     sel->t_bits = T;
     sel->t_key = tkey;
   }
+  __shared__ int8_t sQat[64];
+  if (late) {
+    out_order_par(a.in, kind, a.q, a.gb, sQat);
+    __syncthreads();
+    if (blockIdx.x == 0 && tid < 64) sel->qat[tid] = sQat[tid];
+  }
   // 3. survivors per tile and exact sums
-  count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, sCnt);
+  count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, late, lpre, sQat);
+  if (late) {
+    // 3b. the boundary bin: its threshold pair, then its survivors counted
+    // per tile and their mass added to this block's partial sums
+    if (!grid_sync(a)) return;
+    __shared__ long long sM;
+    __shared__ unsigned long long sTb, sTk;
+    if (tid == 0) sM = *(volatile long long*)&sel->n_cand;
+    __syncthreads();
+    long long m = sM;
+    if (m > a.ws.max_n) {
+      if (blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+      m = a.ws.max_n;
+    }
+    unsigned long long tb, tk;
+    if (m <= kCandSmem) {
+      settle_small(a, smem, m, lneed, &tb, &tk);
+    } else {
+      if (blockIdx.x == 0) {
+        settle_radix(a, smem, m, lneed, lpre, &tb, &tk);
+        if (tid == 0) {
+          sel->t_bits = tb;
+          sel->t_key = tk;
+        }
+      }
+      if (!grid_sync(a)) return;
+      if (tid == 0) {
+        sTb = *(volatile unsigned long long*)&sel->t_bits;
+        sTk = *(volatile unsigned long long*)&sel->t_key;
+      }
+      __syncthreads();
+      tb = sTb;
+      tk = sTk;
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+      sel->t_bits = tb;
+      sel->t_key = tk;
+    }
+    const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;
+    i128 v[3] = {0, 0, 0};
+    for (long long k = (long long)blockIdx.x * blockDim.x + tid; k < m; k += (long long)gridDim.x * blockDim.x) {
+      const unsigned long long i = __ldcg(a.ws.cand_bits + k);
+      const unsigned long long bits = __ldcg(slots + i);
+      if (bits > tb || (bits == tb && __ldcg(a.ws.cand_key + k) <= tk)) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(a.ws.status + tile_of((long long)(i >> lns), kind, a.ws.part)),
+                  1ULL);
+        v[0] += fx_from_pbits(bits);
+        if (P2) {
+          const double p = __longlong_as_double((long long)bits);
+          v[1] += fx_from_pbits((unsigned long long)__double_as_longlong(__dmul_rn(p, p)));
+        }
+      }
+    }
+    block_sum_i128<3>(v, sRed);
+    if (tid == 0) {
+      Partial* pt = a.ws.partials + blockIdx.x;
+      pt->s[0] += v[0];
+      pt->s[1] += v[1];
+    }
+  }
   // 4. sums, decision, tile offsets
   finish_by_last_block(a, kind, mode, j, trace, sRed);
 }
@@ -1597,7 +1496,9 @@ __global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const long long i = i0 + u * kThreads + tid;
-        const bool kept = slot_kept(x[u], T, incl);
+        bool kept = slot_kept(x[u], T, incl);
+        if (!incl && x[u] == T && x[u] != ~0ULL)
+          kept = true_key(__ldcs(a.ws.stage_keys + i), S.qat, 64) <= S.t_key;
         bal[u] = __ballot_sync(0xffffffffu, kept);
         if (kept) {
           kk[u] = __ldcs(a.ws.stage_keys + i);
@@ -1639,15 +1540,7 @@ __global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
     atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_out[kind * 5 + P_WRITE]),
               (unsigned long long)written);
   // the last CTA to finish writes the output descriptor
-  __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    const unsigned long long d = atomicAdd(&reinterpret_cast<unsigned long long*>(a.ws.counters)[59], 1ULL);
-    if (d == gridDim.x - 1) {
-      __threadfence();
-      finalize_op(a, a.tr, a.fin_mode, kind);
-    }
-  }
+  write_done(a, kind);
 }
 
 // Rotation step, after the write pass: keep the candidate if accepted.

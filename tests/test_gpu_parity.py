@@ -159,14 +159,15 @@ def test_topk_large_ties(B, orc):
     assert np.array_equal(st.x, np.sort(xo))
 
 
-@pytest.mark.parametrize("n_tied", [7, 100, 2000])
+@pytest.mark.parametrize("n_tied", [7, 100, 2000, 6000])
 def test_topk_ties_at_threshold(B, orc, n_tied):
     """A run of equal |a|^2 straddling rank k: the survivors among them are the
-    smallest keys.  Tie sizes cover the counting (<= 256), sorting (<= 4096)
-    and radix paths of the exact candidate step."""
+    smallest keys, and the kept mass counts them exactly.  Tie sizes cover the
+    counting (<= 256), sorting (<= 4096) and radix paths of the boundary
+    bin's settle step."""
     from bass_b200 import _native
     rng = np.random.default_rng(9 + n_tied)
-    N, n = 24, 30000
+    N, n = 24, max(30000, 12 * n_tied)
     x = np.unique(rng.integers(0, 2 ** N, size=2 * n, dtype=np.uint64))[:n]
     rng.shuffle(x)
     a = (rng.uniform(0.5, 1.0, n) + 1j * rng.uniform(-0.5, 0.5, n)) / 100.0
@@ -176,10 +177,13 @@ def test_topk_ties_at_threshold(B, orc, n_tied):
     idx = np.flatnonzero(~big)[:n_tied]
     a[idx] = tied
     st = gpu_state(B, N, x, a)
-    st._topk(_native.trunc(k, k))
-    xo, ao, _, _ = orc.select_topk(x, a, k)
+    st._topk(_native.trunc(k, k, 3, 2))           # SparseState.truncate_top_k semantics
+    xo, ao, kept, _ = orc.select_topk(x, a, k)
     assert st.nnz == k
-    assert np.array_equal(st.x, np.sort(xo))
+    xs, as_ = sorted_state(xo, ao)
+    assert np.array_equal(st.x, xs)
+    assert abs(st.gamma - np.sqrt(kept)) <= 1e-15
+    assert np.max(np.abs(st.alpha - as_ / np.sqrt(kept))) < 1e-15
 
 
 def test_rdm_exact(B, orc):
