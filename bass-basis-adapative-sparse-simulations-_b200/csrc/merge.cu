@@ -1153,21 +1153,45 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
       }
     }
     unsigned km = 0;
+    // the chunk's sums as exact integer-valued doubles (fx_split96), folded
+    // into v after the chunk; values of 2 and above take the integer path
+    double dh[3] = {0.0, 0.0, 0.0}, dl[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const bool kept = slot_kept(x[u], T, incl);
       km |= (unsigned)kept << u;
-      if (sums && x[u] != ~0ULL) {
-        const i128 f = fx_from_pbits(x[u]);
-        if (want_total) v[2] += f;
-        if (kept) {
-          v[0] += f;
+      if (sums) {
+        if (x[u] < 0x4000000000000000ULL) {  // 0 <= p < 2
+          const double p = __longlong_as_double((long long)x[u]);
+          double h, l;
+          fx_split96(p, &h, &l);
+          if (want_total) {
+            dh[2] = __dadd_rn(dh[2], h);
+            dl[2] = __dadd_rn(dl[2], l);
+          }
+          dh[0] = __dadd_rn(dh[0], kept ? h : 0.0);
+          dl[0] = __dadd_rn(dl[0], kept ? l : 0.0);
           if (P2) {
-            const double p = __longlong_as_double((long long)x[u]);
-            v[1] += fx_from_pbits((unsigned long long)__double_as_longlong(__dmul_rn(p, p)));
+            fx_split96(kept ? __dmul_rn(p, p) : 0.0, &h, &l);
+            dh[1] = __dadd_rn(dh[1], h);
+            dl[1] = __dadd_rn(dl[1], l);
+          }
+        } else if (x[u] != ~0ULL) {
+          const i128 f = fx_from_pbits(x[u]);
+          if (want_total) v[2] += f;
+          if (kept) {
+            v[0] += f;
+            if (P2) {
+              const double p = __longlong_as_double((long long)x[u]);
+              v[1] += fx_from_pbits((unsigned long long)__double_as_longlong(__dmul_rn(p, p)));
+            }
           }
         }
       }
+    }
+    if (sums) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) v[k] += fx_join96(dh[k], dl[k]);
     }
     // survivors per tile
     const bool live = c < nchunk;
