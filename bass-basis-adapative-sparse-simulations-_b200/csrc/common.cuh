@@ -76,23 +76,6 @@ __device__ __forceinline__ i128 fx_from_pbits(unsigned long long b) {
   return (i128)((u128)m << sh);
 }
 
-// floor(v * 2^96) for 0 <= v < 4 as h * 2^48 + l, with h and l integers
-// below 2^50 and 2^48 held exactly in doubles: x = v * 2^96 and the scalings
-// by 2^-48 and 2^48 are exact (powers of two), x - h * 2^48 is exact (both are
-// multiples of ulp(x), the difference is below 2^48), and truncation to an
-// integer rounds nothing else.  Eight such h (or l) add exactly in a double
-// (every partial sum is an integer below 2^53), so a run of terms is summed in
-// floating point and joined into the 128-bit sum once (fx_join96).
-__device__ __forceinline__ void fx_split96(double v, double* h, double* l) {
-  const double x = __dmul_rn(v, 0x1p96);
-  const double hi = trunc(__dmul_rn(x, 0x1p-48));
-  *h = hi;
-  *l = trunc(__dsub_rn(x, __dmul_rn(hi, 0x1p48)));
-}
-__device__ __forceinline__ i128 fx_join96(double h, double l) {
-  return (i128)(((u128)__double2ull_rz(h) << 48) + (u128)__double2ull_rz(l));
-}
-
 // On the device, for |v| < 2^31 (every probability and moment summed here),
 // the same integer is formed in exact floating-point steps: hi =
 // floor(|v| * 2^32) and lo = floor(frac(|v| * 2^32) * 2^64); both scalings are
@@ -109,6 +92,44 @@ __host__ __device__ __forceinline__ i128 fx_from(double v) {
 #else
   return fx_from_bits(v);
 #endif
+}
+
+// floor(v * 2^96) for 0 <= v < 4 as h * 2^48 + l, with h and l integers
+// below 2^50 and 2^48 held exactly in doubles: x = v * 2^96 and the scalings
+// by 2^-48 and 2^48 are exact (powers of two), x - h * 2^48 is exact (both are
+// multiples of ulp(x), the difference is below 2^48), and truncation to an
+// integer rounds nothing else.  Eight such h (or l) add exactly in a double
+// (every partial sum is an integer below 2^53), so a run of terms is summed in
+// floating point and joined into the 128-bit sum once (fx_join96).
+__device__ __forceinline__ void fx_split96(double v, double* h, double* l) {
+  const double x = __dmul_rn(v, 0x1p96);
+  const double hi = trunc(__dmul_rn(x, 0x1p-48));
+  *h = hi;
+  *l = trunc(__dsub_rn(x, __dmul_rn(hi, 0x1p48)));
+}
+__device__ __forceinline__ i128 fx_join96(double h, double l) {
+  return (i128)(((u128)__double2ull_rz(h) << 48) + (u128)__double2ull_rz(l));
+}
+// Signed form: fx_from(v) for |v| < 2 goes to the split accumulators (h, l)
+// (fx_split96 of |v|, negated for v < 0; at most eight terms before
+// fx_join96s), larger values straight to the 128-bit sum w.
+__device__ __forceinline__ void fx_acc96(double v, double& h, double& l, i128& w) {
+  const double a = fabs(v);
+  if (a < 2.0) {
+    double hh, ll;
+    fx_split96(a, &hh, &ll);
+    if (v < 0.0) {
+      hh = -hh;
+      ll = -ll;
+    }
+    h = __dadd_rn(h, hh);
+    l = __dadd_rn(l, ll);
+  } else {
+    w += fx_from(v);
+  }
+}
+__device__ __forceinline__ i128 fx_join96s(double h, double l) {
+  return (i128)__double2ll_rz(h) * (i128)281474976710656LL + (i128)__double2ll_rz(l);
 }
 
 __device__ __forceinline__ int clz128(u128 u) {

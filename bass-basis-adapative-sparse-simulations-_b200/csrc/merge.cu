@@ -587,25 +587,30 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
     // Round r gives position r * kThreads + tid to thread tid, so neighbouring
     // threads handle neighbouring groups and write neighbouring outputs.
     if (PASS == P_RDM) {
+      // at most kPerThread positions per thread, so at most eight terms per
+      // split accumulator (fx_acc96) before they are joined
       i128 v[4] = {0, 0, 0, 0};
+      double dh[4] = {0.0, 0.0, 0.0, 0.0}, dl[4] = {0.0, 0.0, 0.0, 0.0};
       for (int p = tid; p < E; p += kThreads) {
         const uint64_t z = sZ[p];
         const uint64_t gid = z >> 1;
         if (p > 0 && (sZ[p - 1] >> 1) == gid) continue;
         const double2 x0 = amp(p);
         if ((z & 1ULL) == 0) {
-          v[0] += fx_from(prob(x0));
+          fx_acc96(prob(x0), dh[0], dl[0], v[0]);
           if (p + 1 < E && (sZ[p + 1] >> 1) == gid) {
             const double2 x1 = amp(p + 1);
-            v[1] += fx_from(prob(x1));
+            fx_acc96(prob(x1), dh[1], dl[1], v[1]);
             const double2 c = cmul(x0, make_double2(x1.x, -x1.y));
-            v[2] += fx_from(c.x);
-            v[3] += fx_from(c.y);
+            fx_acc96(c.x, dh[2], dl[2], v[2]);
+            fx_acc96(c.y, dh[3], dl[3], v[3]);
           }
         } else {
-          v[1] += fx_from(prob(x0));
+          fx_acc96(prob(x0), dh[1], dl[1], v[1]);
         }
       }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] += fx_join96s(dh[k], dl[k]);
       block_sum_i128<4>(v, sRed);
       if (tid == 0) {
         Partial* pt = a.ws.partials + (long long)set * a.ws.max_tiles + tile;

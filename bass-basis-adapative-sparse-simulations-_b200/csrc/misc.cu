@@ -19,10 +19,23 @@ __global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsVi
   const double r0 = st->rscale[0], r1 = st->rscale[1];
   const double2* amps = reinterpret_cast<const double2*>(st->amps);
   i128 v[1] = {0};
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const double p = prob(scale_load(amps[i], r0, r1));
-    v[0] += fx_from(MODE == R_NORM2 ? p : __dmul_rn(p, p));
+  // eight entries per thread and round, summed exactly in the split
+  // accumulators (fx_acc96) and joined once per round
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 8 * stride) {
+    double2 x[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const long long i = i0 + u * stride;
+      x[u] = i < n ? amps[i] : make_double2(0.0, 0.0);
+    }
+    double h = 0.0, l = 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const double p = prob(scale_load(x[u], r0, r1));
+      fx_acc96(MODE == R_NORM2 ? p : __dmul_rn(p, p), h, l, v[0]);
+    }
+    v[0] += fx_join96s(h, l);
   }
   block_sum_i128<1>(v, sRed);
   if (threadIdx.x == 0) ws.red[blockIdx.x] = v[0];
