@@ -342,9 +342,12 @@ int bass_rotate_step(bass_state* cur, bass_state* tmp, const double* host_U, int
   tr.k_cond = k;
   tr.k_keep = k;
   tr.trace = trace;
+  // without a trace the write pass commits; with one, the candidate's
+  // fingerprint comes first and k_commit follows it
+  a.commit = trace ? 0 : 1;
   cudaError_t e = run_merge_op(K_ROT1, a, tr, 1, j, s);
   if (e == cudaSuccess && trace) e = run_fingerprint(tmp, kSigPmin, nullptr, v, s, ctrl, 1, 0);
-  if (e == cudaSuccess) e = run_commit(cur, tmp, ctrl, v, j, trace, s);
+  if (e == cudaSuccess && trace) e = run_commit(cur, tmp, ctrl, v, j, trace, s);
   return status_of(e);
 }
 

@@ -28,6 +28,8 @@ struct OpArgs {
   int write_mode; // P_WRITE: 0 look-back + drop rule, 2 one child per entry
   int fin;        // P_WRITE: the last CTA to finish writes the output descriptor (finalize_op)
   int fin_mode;   // finalize_op: 0 gate / truncation, 1 rotation step
+  int commit;     // rotation step: the last CTA of the write pass also commits (swaps in an accepted candidate)
+  int j;          // rotation step: the rotated qubit
   long long k_cond, k_keep;
   bass_trunc tr;  // finalize_op: gamma / renormalisation rules
 };

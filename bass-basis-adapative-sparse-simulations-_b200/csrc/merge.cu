@@ -362,6 +362,33 @@ __device__ void write_done(const OpArgs& a, int kind) {
     a.out->qat[threadIdx.x] = sQo[threadIdx.x];
     a.out->pos[sQo[threadIdx.x]] = (int8_t)threadIdx.x;
   }
+  if (!a.commit) return;
+  // rotation step without a trace: k_commit's work, here.  An accepted
+  // candidate (a.out) becomes the state (a.in): the two descriptors are
+  // swapped one 8-byte word per thread.
+  __syncthreads();
+  const volatile SelState* sel = a.ws.sel;
+  if (!sel->accept) return;
+  constexpr int kWords = (int)(sizeof(bass_state) / 8);
+  static_assert(sizeof(bass_state) % 8 == 0, "descriptor words");
+  unsigned long long* pc = reinterpret_cast<unsigned long long*>(const_cast<bass_state*>(a.in));
+  unsigned long long* pt = reinterpret_cast<unsigned long long*>(a.out);
+  unsigned long long wc = 0, wt = 0;
+  if (threadIdx.x < kWords) {
+    wc = pc[threadIdx.x];
+    wt = pt[threadIdx.x];
+  }
+  __syncthreads();
+  if (threadIdx.x < kWords) {
+    pc[threadIdx.x] = wt;
+    pt[threadIdx.x] = wc;
+  }
+  if (threadIdx.x == 0) {
+    bass_ctrl* c = a.ctrl;
+    c->pr_cur = sel->pr_new;
+    const double frac = c->frac[a.j];
+    c->gamma_running *= sqrt(frac > 1e-30 ? frac : 0.0);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1694,6 +1721,7 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
   a.fin = 1;
   a.fin_mode = fin_mode;
   a.tr = tr;
+  a.j = j;
   if constexpr (KIND == K_PERM) {
     a.write_mode = 2;
     return launch_tile<KIND, P_WRITE>(a, 3, s, nullptr);
