@@ -314,6 +314,60 @@ __device__ __forceinline__ void warp_lower_bound3(const uint64_t* keys, long lon
   }
 }
 
+// One galloping round before warp_lower_bound3, for three searches whose
+// answers lie near a known position P: lanes 10k .. 10k + 9 probe P -/+ 4^l
+// (l = 0..9) for search k, backwards when back[k] (the answer is at or before
+// P) and forwards otherwise (the answer is after P), and [lo[k], hi[k]) shrinks
+// to the bracket between the nearest probe on the far side of the answer and
+// the one before it.  Probes outside [lo[k], hi[k]) count as far side and
+// load nothing.  Called by all 32 lanes of a warp.
+__device__ __forceinline__ void warp_bracket3(const uint64_t* keys, long long P, long long (&lo)[3],
+                                              long long (&hi)[3], const uint64_t (&thr)[3],
+                                              const bool (&back)[3]) {
+  const int lane = threadIdx.x & 31;
+  const int k = lane / 10, l = lane - 10 * k;
+  bool far = false;
+#pragma unroll
+  for (int kk = 0; kk < 3; ++kk) {
+    if (k == kk) {
+      const long long d = 1LL << (2 * l);
+      if (back[kk]) {
+        const long long pos = P - d;
+        far = pos < lo[kk] || keys[pos] < thr[kk];
+      } else {
+        const long long pos = P + d;
+        far = pos >= hi[kk] || keys[pos] >= thr[kk];
+      }
+    }
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, far);
+#pragma unroll
+  for (int kk = 0; kk < 3; ++kk) {
+    const unsigned mk = (m >> (10 * kk)) & 0x3FFu;
+    long long nlo, nhi;
+    if (mk) {
+      const int l0 = __ffs(mk) - 1;
+      const long long dfar = 1LL << (2 * l0), dnear = l0 ? 1LL << (2 * (l0 - 1)) : 0;
+      if (back[kk]) {
+        nlo = P - dfar + 1;
+        nhi = P - dnear + 1;
+      } else {
+        nlo = P + dnear + 1;
+        nhi = P + dfar + 1;
+      }
+    } else if (back[kk]) {
+      nlo = lo[kk];
+      nhi = P - (1LL << 18) + 1;
+    } else {
+      nlo = P + (1LL << 18) + 1;
+      nhi = hi[kk];
+    }
+    if (nlo > lo[kk]) lo[kk] = nlo;
+    if (nhi < hi[kk]) hi[kk] = nhi;
+    if (lo[kk] > hi[kk]) lo[kk] = hi[kk];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // decoupled look-back (exclusive prefix of per-tile counts)
 // status word: bits 62-63 flag (1 aggregate, 2 inclusive), bits 0-61 value

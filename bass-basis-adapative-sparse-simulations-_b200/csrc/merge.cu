@@ -98,6 +98,8 @@ __global__ void k_partition(OpArgs a, int kind) {
       long long lo3[3] = {0, ((y >> t) & 1ULL) ? 0 : P + 1, hi_ovf ? n : P + 1};
       long long hi3[3] = {P + 1, ((y >> t) & 1ULL) ? P + 1 : n, n};
       const uint64_t thr3[3] = {lo_key, mid_key, hi_key};
+      const bool back3[3] = {true, ((y >> t) & 1ULL) != 0, false};
+      warp_bracket3(keys, P, lo3, hi3, thr3, back3);
       warp_lower_bound3(keys, lo3, hi3, thr3);
       const long long s = lo3[0], mid = lo3[1], e = lo3[2];
       const long long d = P - s, len0 = mid - s, len1 = e - mid;
