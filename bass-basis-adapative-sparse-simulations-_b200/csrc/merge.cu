@@ -65,8 +65,17 @@ __device__ __forceinline__ void out_order_par(const bass_state* in, int kind, in
 // partition
 // ---------------------------------------------------------------------------
 // record per boundary: P' (adjusted Z position), s, mid, e (block bounds), i, j
-__global__ void k_partition(OpArgs a, int kind) {
+// zero: also clear the op's small workspace region (what zero_small clears);
+// nothing here reads it, and the kernels after the partition find it zeroed.
+__global__ void k_partition(OpArgs a, int kind, int zero) {
   const int set = blockIdx.y;
+  if (zero && set == 0) {
+    unsigned long long* zp = reinterpret_cast<unsigned long long*>(a.ws.counters);
+    const long long nw =
+        (long long)((reinterpret_cast<const char*>(a.ws.status + a.ws.max_tiles) - reinterpret_cast<const char*>(zp)) / 8);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x)
+      zp[i] = 0ULL;
+  }
   const bass_state* in = a.in;
   const long long n = in->nnz;
   const int q = (kind == K_RDM) ? set : a.q;
@@ -1706,13 +1715,15 @@ static cudaError_t launch_select(OpArgs a, int ns, int kind, int gh, int mode, i
 
 template <int KIND>
 static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j, cudaStream_t s) {
-  cudaError_t e = zero_small(a.ws, s);
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
   a.k_cond = tr.k_cond;
   a.k_keep = tr.k_keep;
   a.nsets = 1;
   if constexpr (KIND != K_IDENT) {
-    KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, 1), 256, 0, s>>>(a, KIND));
+    // the partition also clears the small workspace region
+    KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, 1), 256, 0, s>>>(a, KIND, 1));
+  } else {
+    if ((e = zero_small(a.ws, s)) != cudaSuccess) return e;
   }
   if constexpr (KIND != K_PERM) {
     constexpr int ns = slots_per_entry(KIND);
@@ -1772,7 +1783,7 @@ cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, 
   a.q = 0;
   a.gb = 0;
   a.nsets = nq;
-  KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, nq), 256, 0, s>>>(a, K_RDM));
+  KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, nq), 256, 0, s>>>(a, K_RDM, 0));
   if ((e = launch_tile<K_RDM, P_RDM>(a, 0, s, nullptr)) != cudaSuccess) return e;
   KLAUNCH(S_RDM_FINAL, s, k_rdm_final<<<nq, 256, 0, s>>>(st, rho, ws, 0));
   return cudaGetLastError();
@@ -1818,7 +1829,7 @@ cudaError_t run_rdm_prepared(const bass_state* st, int nq, double* rho, bass_ctr
   a.q = 0;
   a.gb = 0;
   a.nsets = nq;
-  KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, nq), 256, 0, s>>>(a, K_RDM));
+  KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, nq), 256, 0, s>>>(a, K_RDM, 0));
   cudaError_t e = launch_tile<K_RDM, P_RDM>(a, 0, s, nullptr);
   if (e != cudaSuccess) return e;
   KLAUNCH(S_RDM_FINAL, s, k_rdm_final_bounded<<<nq, 256, 0, s>>>(st, rho, ws, ctrl));
