@@ -314,6 +314,13 @@ __device__ __forceinline__ void warp_lower_bound3(const uint64_t* keys, long lon
   }
 }
 
+// Programmatic dependent launch (launch_pdl): wait until the previous
+// kernel of the stream has completed and its memory is visible; signal that
+// this block's part of the grid no longer needs its SM to itself, so the next
+// kernel may be scheduled.  Both are no-ops for a kernel launched normally.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // One galloping round before warp_lower_bound3, for three searches whose
 // answers lie near a known position P: lanes 10k .. 10k + 9 probe P -/+ 4^l
 // (l = 0..9) for search k, backwards when back[k] (the answer is at or before

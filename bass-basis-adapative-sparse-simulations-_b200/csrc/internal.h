@@ -1,6 +1,7 @@
 // internal.h -- host-side launchers shared by the .cu files of libbass_b200.
 #pragma once
 
+#include <utility>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -56,6 +57,26 @@ bool prof_on();
     ::bass::ProfScope _ps((slot), (stream)); \
     __VA_ARGS__;                          \
   } while (0)
+
+// Launch with programmatic dependent launch: the grid may be scheduled while
+// the previous kernel of the stream finishes (after every block of that
+// kernel has called pdl_trigger or exited).  The kernel must call pdl_wait
+// before it touches any memory, so only the launch itself overlaps.
+template <typename... K, typename... A>
+inline cudaError_t launch_pdl(void (*kern)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
 
 struct Device {
   int sms;

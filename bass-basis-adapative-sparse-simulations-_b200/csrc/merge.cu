@@ -68,6 +68,7 @@ __device__ __forceinline__ void out_order_par(const bass_state* in, int kind, in
 // zero: also clear the op's small workspace region (what zero_small clears);
 // nothing here reads it, and the kernels after the partition find it zeroed.
 __global__ void k_partition(OpArgs a, int kind, int zero) {
+  pdl_wait();
   const int set = blockIdx.y;
   if (zero && set == 0) {
     unsigned long long* zp = reinterpret_cast<unsigned long long*>(a.ws.counters);
@@ -146,6 +147,7 @@ __global__ void k_partition(OpArgs a, int kind, int zero) {
       r[0] = r0; r[1] = r1; r[2] = r2; r[3] = r3; r[4] = r4; r[5] = r5;
     }
   }
+  pdl_trigger();
 }
 
 // ---------------------------------------------------------------------------
@@ -412,6 +414,7 @@ __device__ void write_done(const OpArgs& a, int kind) {
 // moments).
 template <int KIND, int PASS>
 __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   double2* sA = reinterpret_cast<double2*>(smem);
   uint64_t* sZ = reinterpret_cast<uint64_t*>(sA + kTilePad);
@@ -775,6 +778,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
     __syncthreads();
   }
 
+  pdl_trigger();
   // ---- write pass: the last CTA to finish writes the output descriptor ------
   if (PASS == P_WRITE && a.fin) write_done(a, KIND);
 
@@ -1506,6 +1510,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
     }
   }
   // 4. sums, decision, tile offsets
+  pdl_trigger();
   finish_by_last_block(a, kind, mode, j, trace, sRed);
 }
 
@@ -1519,6 +1524,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
 // slots per thread and round.  The last CTA to finish writes the output
 // descriptor.  A rejected rotation candidate is not written.
 __global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
+  pdl_wait();
   __shared__ SelState S;
   __shared__ int sCnt[8][kThreads / 32];  // survivors per (round u, warp)
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -1607,6 +1613,7 @@ __global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
     atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_out[kind * 5 + P_WRITE]),
               (unsigned long long)written);
   // the last CTA to finish writes the output descriptor
+  pdl_trigger();
   write_done(a, kind);
 }
 
@@ -1672,7 +1679,7 @@ static cudaError_t launch_tile(OpArgs a, int counter, cudaStream_t s, int* grid_
   }
   a.counter = counter;
   a.prof = prof_on() ? 1 : 0;
-  KLAUNCH(KIND * 5 + PASS, s, k_tile<KIND, PASS><<<grid, kThreads, smem, s>>>(a));
+  KLAUNCH(KIND * 5 + PASS, s, launch_pdl(k_tile<KIND, PASS>, dim3(grid), dim3(kThreads), smem, s, a));
   if (grid_out) *grid_out = grid;
   return cudaGetLastError();
 }
@@ -1721,7 +1728,7 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
   a.nsets = 1;
   if constexpr (KIND != K_IDENT) {
     // the partition also clears the small workspace region
-    KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, 1), 256, 0, s>>>(a, KIND, 1));
+    KLAUNCH(S_PARTITION, s, launch_pdl(k_partition, dim3(device().grid_small, 1), dim3(256), 0, s, a, (int)KIND, 1));
   } else {
     if ((e = zero_small(a.ws, s)) != cudaSuccess) return e;
   }
@@ -1741,7 +1748,8 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
   } else {
     a.prof = prof_on() ? 1 : 0;
     KLAUNCH(KIND * 5 + P_WRITE, s,
-            k_compact<<<device().sms * 4, kThreads, 0, s>>>(a, slots_per_entry(KIND), KIND));
+            launch_pdl(k_compact, dim3(device().sms * 4), dim3(kThreads), 0, s, a, (int)slots_per_entry(KIND),
+                       (int)KIND));
     return cudaGetLastError();
   }
 }
