@@ -16,7 +16,7 @@
 //                 evaluates every group (gate / rotation / permutation / RDM
 //                 moments); the evaluation pass stages every child (|a|^2 bit
 //                 pattern, key, amplitude) at its slot index;
-//   k_select_coop cooperative selection: radix select of the top-k threshold
+//   k_select_coop one-launch selection (grid barriers): radix select of the top-k threshold
 //                 on the IEEE bits of |a|^2 (13-bit digits, then an exact
 //                 (|a|^2 desc, key asc) ordering of the boundary candidates),
 //                 survivors per tile, exact sums, rotation decision, tile scan;
@@ -797,7 +797,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// selection: one cooperative launch per op
+// selection: one launch per op, every block resident (grid barriers)
 // ---------------------------------------------------------------------------
 // After the evaluation pass has written every child's |a|^2 bit pattern to the
 // slot array (NS words per Z position, ~0 where a group has fewer children),
@@ -824,8 +824,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
 // workspace with a bounded spin (BASS_ERR_WAIT, then every block returns).
 constexpr int kSelThreads = 512;
 
-// Grid-wide barrier of a cooperative launch.  Returns false (error recorded)
-// if the wait gave up.
+// Grid-wide barrier of the selection's grid (every block resident, see
+// launch_select_t).  Returns false (error recorded) if the wait gave up.
 __device__ bool grid_sync(const OpArgs& a) {
   __shared__ int sOk;
   __syncthreads();
@@ -1367,6 +1367,7 @@ __device__ void finish_by_last_block(const OpArgs& a, int kind, int mode, int j,
 template <bool P2>
 __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, int kind, int nblk_hist, int mode,
                                                               int j, int trace) {
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned int* h = reinterpret_cast<unsigned int*>(smem);
   __shared__ long long sS[kSelThreads / 32];
@@ -1690,7 +1691,10 @@ cudaError_t zero_small(const WsView& ws, cudaStream_t s) {
   return cudaMemsetAsync(ws.counters, 0, bytes, s);
 }
 
-// Cooperative launch of the selection; grid = every co-resident block.
+// Launch of the selection; grid = every block that fits on the GPU at once
+// (its grid barriers need them all resident).  It is a programmatic
+// dependent launch: each block waits until the evaluation pass has completed,
+// and by then that pass has left every SM, so all blocks fit together.
 template <bool P2>
 static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace,
                                    cudaStream_t s) {
@@ -1710,8 +1714,7 @@ static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode,
   a.prof = prof_on() ? 1 : 0;
   dim3 grd(grid), blk(kSelThreads);
   cudaError_t e = cudaSuccess;
-  void* args[] = {&a, &ns, &kind, &gh, &mode, &j, &trace};
-  KLAUNCH(S_SELECT1, s, e = cudaLaunchCooperativeKernel((const void*)k_select_coop<P2>, grd, blk, args, smem, s));
+  KLAUNCH(S_SELECT1, s, e = launch_pdl(k_select_coop<P2>, grd, blk, smem, s, a, ns, kind, gh, mode, j, trace));
   return e;
 }
 
@@ -1781,8 +1784,7 @@ cudaError_t run_ident_write(OpArgs a, cudaStream_t s) {
 
 cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
                     cudaStream_t s) {
-  cudaError_t e = zero_small(ws, s);
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
   OpArgs a{};
   a.in = st;
   a.out = nullptr;
@@ -1791,7 +1793,8 @@ cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, 
   a.q = 0;
   a.gb = 0;
   a.nsets = nq;
-  KLAUNCH(S_PARTITION, s, k_partition<<<dim3(device().grid_small, nq), 256, 0, s>>>(a, K_RDM, 0));
+  // the partition also clears the small workspace region
+  KLAUNCH(S_PARTITION, s, launch_pdl(k_partition, dim3(device().grid_small, nq), dim3(256), 0, s, a, (int)K_RDM, 1));
   if ((e = launch_tile<K_RDM, P_RDM>(a, 0, s, nullptr)) != cudaSuccess) return e;
   KLAUNCH(S_RDM_FINAL, s, k_rdm_final<<<nq, 256, 0, s>>>(st, rho, ws, 0));
   return cudaGetLastError();
