@@ -1567,12 +1567,21 @@ __global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
       unsigned bal[8];
       unsigned long long kk[8];
       double2 aa[8];
+      unsigned km = 0, tm = 0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        km |= (unsigned)slot_kept(x[u], T, incl) << u;
+        tm |= (unsigned)(!incl && x[u] == T && x[u] != ~0ULL) << u;
+      }
+      // children tied at the threshold pattern: kept up to the true key t_key
+      for (unsigned r = tm; r; r &= r - 1) {
+        const int u = __ffs(r) - 1;
+        if (true_key(__ldcs(a.ws.stage_keys + i0 + u * kThreads + tid), S.qat, 64) <= S.t_key) km |= 1u << u;
+      }
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const long long i = i0 + u * kThreads + tid;
-        bool kept = slot_kept(x[u], T, incl);
-        if (!incl && x[u] == T && x[u] != ~0ULL)
-          kept = true_key(__ldcs(a.ws.stage_keys + i), S.qat, 64) <= S.t_key;
+        const bool kept = (km >> u) & 1u;
         bal[u] = __ballot_sync(0xffffffffu, kept);
         if (kept) {
           kk[u] = __ldcs(a.ws.stage_keys + i);
