@@ -404,6 +404,16 @@ __device__ void write_done(const OpArgs& a, int kind) {
   }
 }
 
+// The selection state into shared memory, one 8-byte word per thread (the
+// caller synchronises before reading it).
+__device__ __forceinline__ void load_sel(SelState* dst, const SelState* src) {
+  constexpr int kWords = (int)(sizeof(SelState) / 8);
+  static_assert(sizeof(SelState) % 8 == 0, "selection state words");
+  if ((int)threadIdx.x < kWords)
+    reinterpret_cast<unsigned long long*>(dst)[threadIdx.x] =
+        __ldcg(reinterpret_cast<const unsigned long long*>(src) + threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // the tile kernel
 // ---------------------------------------------------------------------------
@@ -433,7 +443,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
 
   const int tid = threadIdx.x;
   if (tid < 16) sG[tid] = a.G[tid];
-  if (tid == 0) S = *a.ws.sel;
+  load_sel(&S, a.ws.sel);
   __syncthreads();
   if (KIND == K_IDENT && a.guard && S.pad == 0) return;
   // a rejected rotation candidate is not written (the descriptor still is)
@@ -1529,7 +1539,7 @@ __global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
   __shared__ SelState S;
   __shared__ int sCnt[8][kThreads / 32];  // survivors per (round u, warp)
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  if (tid == 0) S = *a.ws.sel;
+  load_sel(&S, a.ws.sel);
   __syncthreads();
   const long long n = a.in->nnz;
   const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
