@@ -1600,26 +1600,28 @@ __global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
         if (lane == 0) sCnt[u][w] = __popc(bal[u]);
       }
       __syncthreads();
-      int tot = 0;  // survivors of the round
+      // the 64 survivor counts in slot order (round major, warp minor): every
+      // warp scans them itself, lane l holding entries 2l and 2l + 1
+      static_assert(8 * (kThreads / 32) == 64, "two counts per lane");
+      const int* fc = &sCnt[0][0];
+      const int c0 = fc[2 * lane], c1 = fc[2 * lane + 1];
+      int inc = c0 + c1;
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-#pragma unroll
-        for (int v = 0; v < kThreads / 32; ++v) tot += sCnt[u][v];
+      for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += y;
+      }
+      const int tot = __shfl_sync(0xffffffffu, inc, 31);  // survivors of the round
+      const int mine = (w & 1) ? inc - c1 : inc - c0 - c1;  // offset of entry 2l + (w & 1)
       if (base + tot <= cap) {
-        int run = 0;
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-          int ahead = run;
-#pragma unroll
-          for (int v = 0; v < kThreads / 32; ++v)
-            if (v < w) ahead += sCnt[u][v];
+          const int ahead = __shfl_sync(0xffffffffu, mine, u * 4 + (w >> 1));  // entry 8u + w
           if ((bal[u] >> lane) & 1u) {
             const long long o = base + ahead + __popc(bal[u] & lt);
             okeys[o] = kk[u];
             oamps[o] = aa[u];
           }
-#pragma unroll
-          for (int v = 0; v < kThreads / 32; ++v) run += sCnt[u][v];
         }
       } else if (tid == 0) {
         set_error(a.ctrl, BASS_ERR_CAPACITY);
