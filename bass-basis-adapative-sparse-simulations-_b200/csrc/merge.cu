@@ -219,9 +219,13 @@ struct AmpView {
   }
 };
 
+// The children of the group that starts at Z position p (0 if p does not
+// start one).  G is the op's gate matrix, read from the kernel's parameter
+// block (k_tile takes its arguments as a __grid_constant__), so every lane
+// loads the same constant-bank words.
 template <int KIND>
 __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t* sZ, const AmpView& sA, int gb,
-                                                   const double2* sG, int drop_zero, uint64_t* base,
+                                                   const double2* G, int drop_zero, uint64_t* base,
                                                    double2* ca) {
   constexpr int NC = KindTraits<KIND>::kMaxChildren;
   const uint64_t z = sZ[p];
@@ -254,7 +258,7 @@ __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t*
 #pragma unroll
       for (int r = 0; r < NC; ++r) {
         if (lr[r] < 0) continue;
-        const double2 pr = cmul(sG[o * NC + lr[r]], ar[r]);
+        const double2 pr = cmul(G[o * NC + lr[r]], ar[r]);
         if (!cnz(pr)) continue;
         acc = have ? cadd(acc, pr) : pr;
         have = true;
@@ -268,7 +272,7 @@ __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t*
     const double2 a1 = (lr[0] == 1) ? ar[0] : (lr[1] == 1 ? ar[1] : zero);
 #pragma unroll
     for (int o = 0; o < 2; ++o) {
-      const double2 c = cadd(cmul(sG[o * 2], a0), cmul(sG[o * 2 + 1], a1));
+      const double2 c = cadd(cmul(G[o * 2], a0), cmul(G[o * 2 + 1], a1));
       ca[o] = c;
       if (above_drop(c)) mask |= 1u << o;
     }
@@ -423,7 +427,7 @@ __device__ __forceinline__ void load_sel(SelState* dst, const SelState* src) {
 // entry, and the compaction after a diagonal 1-qubit gate), P_RDM (per-qubit
 // moments).
 template <int KIND, int PASS>
-__global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ OpArgs a) {
   pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   double2* sA = reinterpret_cast<double2*>(smem);
@@ -439,10 +443,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
   __shared__ long long sSegLo[5], sSegOff[6];
   __shared__ int sWarp[32];
   __shared__ i128 sRed[4 * (kThreads / 32)];
-  __shared__ double2 sG[16];
 
   const int tid = threadIdx.x;
-  if (tid < 16) sG[tid] = a.G[tid];
   load_sel(&S, a.ws.sel);
   __syncthreads();
   if (KIND == K_IDENT && a.guard && S.pad == 0) return;
@@ -683,7 +685,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
         if (wmode == 2) {
           mk = 1u;
         } else {
-          const unsigned cm = group_children<KIND>(p, E, sZ, amp, gb, sG, a.drop_zero, &kb, ca);
+          const unsigned cm = group_children<KIND>(p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
           if ((cm & 1u) && keep_child((uint64_t)__double_as_longlong(prob(ca[0])), kb, S, H.qat_out)) mk = 1u;
         }
         sMask[p] = (uint8_t)mk;
@@ -731,7 +733,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
           const unsigned mk = sMask[p];
           if (!mk) continue;
           long long o = sBase + sOff[p];
-          group_children<KIND>(p, E, sZ, amp, gb, sG, a.drop_zero, &kb, ca);
+          group_children<KIND>(p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
 #pragma unroll
           for (int c = 0; c < MC; ++c) {
             if ((mk >> c) & 1u) {
@@ -752,7 +754,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(OpArgs a) {
       uint64_t* skeys = a.ws.stage_keys + NS * sZstart;
       double2* samps = a.ws.tmp_amps + NS * sZstart;
       for (int p = tid; p < E; p += kThreads) {
-        const unsigned cm = group_children<KIND>(p, E, sZ, amp, gb, sG, a.drop_zero, &kb, ca);
+        const unsigned cm = group_children<KIND>(p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
         unsigned long long sb[NS];
 #pragma unroll
         for (int c = 0; c < NS; ++c) {
