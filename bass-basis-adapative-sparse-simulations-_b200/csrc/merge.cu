@@ -67,7 +67,7 @@ __device__ __forceinline__ void out_order_par(const bass_state* in, int kind, in
 // record per boundary: P' (adjusted Z position), s, mid, e (block bounds), i, j
 // zero: also clear the op's small workspace region (what zero_small clears);
 // nothing here reads it, and the kernels after the partition find it zeroed.
-__global__ void k_partition(OpArgs a, int kind, int zero) {
+__global__ void k_partition(const __grid_constant__ OpArgs a, int kind, int zero) {
   pdl_wait();
   const int set = blockIdx.y;
   if (zero && set == 0) {
@@ -1377,7 +1377,7 @@ __device__ void finish_by_last_block(const OpArgs& a, int kind, int mode, int j,
 
 // nblk_hist: CTAs of the evaluation pass (per-CTA child counts in partials c[0]).
 template <bool P2>
-__global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, int kind, int nblk_hist, int mode,
+__global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_constant__ OpArgs a, int ns, int kind, int nblk_hist, int mode,
                                                               int j, int trace) {
   pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1536,7 +1536,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(OpArgs a, int ns, i
 // tile's base (the selection's scan of the tile counts) on, eight consecutive
 // slots per thread and round.  The last CTA to finish writes the output
 // descriptor.  A rejected rotation candidate is not written.
-__global__ void __launch_bounds__(256) k_compact(OpArgs a, int ns, int kind) {
+__global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs a, int ns, int kind) {
   pdl_wait();
   __shared__ SelState S;
   __shared__ int sCnt[8][kThreads / 32];  // survivors per (round u, warp)
