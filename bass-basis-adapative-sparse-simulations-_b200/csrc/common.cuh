@@ -233,16 +233,6 @@ __device__ __forceinline__ uint64_t true_key(uint64_t y, const int8_t* qat, int 
   (void)nq;
   return x;
 }
-// true key -> physical key, given pos[q]
-__device__ __forceinline__ uint64_t phys_key(uint64_t x, const int8_t* pos) {
-  uint64_t y = 0;
-  while (x) {
-    int q = __ffsll((long long)x) - 1;
-    y |= 1ULL << pos[q];
-    x &= x - 1;
-  }
-  return y;
-}
 
 // Move physical bit t down to bit position gb (bits gb..t-1 shift up by one).
 // For gb = 0 this is "target to the lowest bit"; for gb = 1 bit 0 stays.
@@ -458,14 +448,6 @@ __device__ __forceinline__ long long lookback_warp(unsigned long long* status, l
   return excl;
 }
 
-// warp-aggregated shared-memory histogram increment; every lane of the warp
-// must call it (valid = false for lanes with nothing to add)
-__device__ __forceinline__ void hist_add(unsigned int* h, unsigned bin, bool valid) {
-  const unsigned key = valid ? bin : 0xFFFFFFFFu;
-  const unsigned peers = __match_any_sync(0xffffffffu, key);
-  const int lane = threadIdx.x & 31;
-  if (valid && (__ffs(peers) - 1) == lane) atomicAdd(&h[bin], (unsigned)__popc(peers));
-}
 
 // ---------------------------------------------------------------------------
 // workspace
