@@ -509,6 +509,100 @@ int64_t orc_rotate_1q(const uint64_t* x, const cd* a, int64_t nnz, int qubit, co
   return n;
 }
 
+/* Groups of entries that agree on every bit except q1 and q2, ascending by
+   the remaining bits: g[4 * t + idx] = entry index or -1, idx = (bit_q1 << 1)
+   | bit_q2.  Returns the number of groups (or -2), bases in base_out. */
+static int64_t groups_2q(const uint64_t* x, int64_t nnz, int q1, int q2, int64_t** g_out,
+                         uint64_t** base_out) {
+  uint64_t m12 = (1ULL << q1) | (1ULL << q2);
+  ri* v = (ri*)malloc((size_t)(nnz > 0 ? nnz : 1) * sizeof(ri));
+  int64_t* g = (int64_t*)malloc((size_t)(nnz > 0 ? nnz : 1) * 4 * sizeof(int64_t));
+  uint64_t* b = (uint64_t*)malloc((size_t)(nnz > 0 ? nnz : 1) * sizeof(uint64_t));
+  if (!v || !g || !b) { free(v); free(g); free(b); return -2; }
+  for (int64_t i = 0; i < nnz; ++i) { v[i].r = x[i] & ~m12; v[i].i = i; }
+  qsort(v, (size_t)nnz, sizeof(ri), ri_cmp);
+  int64_t ng = 0, i = 0;
+  while (i < nnz) {
+    uint64_t r = v[i].r;
+    for (int t = 0; t < 4; ++t) g[4 * ng + t] = -1;
+    while (i < nnz && v[i].r == r) {
+      int64_t oi = v[i].i;
+      int idx = (int)((((x[oi] >> q1) & 1ULL) << 1) | ((x[oi] >> q2) & 1ULL));
+      g[4 * ng + idx] = oi;
+      ++i;
+    }
+    b[ng++] = r;
+  }
+  free(v);
+  *g_out = g;
+  *base_out = b;
+  return ng;
+}
+
+/* bass_simulator.py:200-231  compute_2qubit_rdm: 4x4 rho (row-major), index
+   (bit_q1 << 1) | bit_q2; over the groups of entries that share every other
+   bit, rho[p][q] += a_p * conj(a_q).  Exact sums (the reference sums in
+   group order in floating point). */
+int orc_rdm_2q(const uint64_t* x, const cd* a, int64_t nnz, int q1, int q2, cd* rho) {
+  int64_t* g;
+  uint64_t* b;
+  int64_t ng = groups_2q(x, nnz, q1, q2, &g, &b);
+  if (ng < 0) return -2;
+  i128 acc[16][2];
+  memset(acc, 0, sizeof(acc));
+  const cd zero = {0.0, 0.0};
+  for (int64_t t = 0; t < ng; ++t) {
+    cd v[4];
+    for (int k = 0; k < 4; ++k) v[k] = g[4 * t + k] >= 0 ? a[g[4 * t + k]] : zero;
+    for (int p = 0; p < 4; ++p)
+      for (int q = 0; q < 4; ++q) {
+        cd cq = {v[q].re, -v[q].im};
+        cd c = cd_mul(v[p], cq);
+        acc[4 * p + q][0] += fx_from(c.re);
+        acc[4 * p + q][1] += fx_from(c.im);
+      }
+  }
+  for (int k = 0; k < 16; ++k) { rho[k].re = fx_to(acc[k][0]); rho[k].im = fx_to(acc[k][1]); }
+  free(g); free(b);
+  return 0;
+}
+
+/* bass_simulator.py:237-289  apply_2qubit_rotation_sparse: per group,
+   a_out[o] = sum over the present inputs of U4[o][idx] * a_in[idx] (ascending
+   idx, exact-zero products skipped as in the 2-qubit gate), children with
+   |a_out| <= 1e-30 dropped.  Output key-sorted; x_out/a_out hold 4*nnz. */
+int64_t orc_rotate_2q(const uint64_t* x, const cd* a, int64_t nnz, int q1, int q2, const cd* U4,
+                      uint64_t* x_out, cd* a_out) {
+  int64_t* g;
+  uint64_t* b;
+  int64_t ng = groups_2q(x, nnz, q1, q2, &g, &b);
+  if (ng < 0) return -2;
+  uint64_t m1 = 1ULL << q1, m2 = 1ULL << q2;
+  int64_t n = 0;
+  for (int64_t t = 0; t < ng; ++t) {
+    for (int o = 0; o < 4; ++o) {
+      int have = 0;
+      cd acc = {0.0, 0.0};
+      for (int k = 0; k < 4; ++k) {
+        if (g[4 * t + k] < 0) continue;
+        cd c = cd_mul(U4[o * 4 + k], a[g[4 * t + k]]);
+        if (!cd_nz(c)) continue;
+        acc = have ? cd_add(acc, c) : c;
+        have = 1;
+      }
+      if (hypot(acc.re, acc.im) > 1e-30) {
+        uint64_t xn = b[t];
+        if ((o >> 1) & 1) xn |= m1;
+        if (o & 1) xn |= m2;
+        x_out[n] = xn; a_out[n] = acc; ++n;
+      }
+    }
+  }
+  free(g); free(b);
+  if (orc_radix_sort(x_out, a_out, n)) return -2;
+  return n;
+}
+
 /* ------------------------------------------------------------------ */
 /* reductions and fingerprints                                          */
 /* ------------------------------------------------------------------ */

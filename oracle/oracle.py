@@ -77,6 +77,8 @@ def lib():
             "orc_rdm_all": (I, [P, P, I64, I, P]),
             "orc_eigh_2x2": (None, [P, P, P]),
             "orc_rotate_1q": (I64, [P, P, I64, I, P, P, P]),
+            "orc_rdm_2q": (I, [P, P, I64, I, I, P]),
+            "orc_rotate_2q": (I64, [P, P, I64, I, I, P, P, P]),
             "orc_sum_p": (D, [P, I64]),
             "orc_sum_p2": (D, [P, I64]),
             "orc_fingerprint": (None, [P, P, I64, D, P]),
@@ -212,6 +214,27 @@ def rotate_1q(x, a, qubit, U):
     x = np.ascontiguousarray(x, dtype=U64); a = _c(a); U = _c(U)
     xo = np.empty(2 * len(x) + 1, U64); ao = np.empty(2 * len(x) + 1, C128)
     n = lib().orc_rotate_1q(_p(x), _p(a), len(x), int(qubit), _p(U), _p(xo), _p(ao))
+    if n < 0:
+        raise MemoryError
+    return xo[:n].copy(), ao[:n].copy()
+
+
+def rdm_2q(x, a, q1, q2):
+    """bass_simulator.py:200-231 compute_2qubit_rdm -> complex (4, 4), index
+    (bit_q1 << 1) | bit_q2; exact sums."""
+    x = np.ascontiguousarray(x, dtype=U64); a = _c(a)
+    rho = np.zeros((4, 4), C128)
+    if lib().orc_rdm_2q(_p(x), _p(a), len(x), int(q1), int(q2), _p(rho)):
+        raise MemoryError
+    return rho
+
+
+def rotate_2q(x, a, q1, q2, U4):
+    """bass_simulator.py:237-289 apply_2qubit_rotation_sparse (returns new,
+    key-sorted arrays)."""
+    x = np.ascontiguousarray(x, dtype=U64); a = _c(a); U4 = _c(U4)
+    xo = np.empty(4 * len(x) + 1, U64); ao = np.empty(4 * len(x) + 1, C128)
+    n = lib().orc_rotate_2q(_p(x), _p(a), len(x), int(q1), int(q2), _p(U4), _p(xo), _p(ao))
     if n < 0:
         raise MemoryError
     return xo[:n].copy(), ao[:n].copy()
@@ -372,15 +395,14 @@ def eigh_2x2_py(rho):
 
 
 class OracleBASS:
-    """bass_simulator.py:478-929 (1-qubit coordinate descent; the optional
-    2-qubit passes are not restated)."""
+    """bass_simulator.py:478-929: 1-qubit coordinate descent and, with
+    use_2qubit_rotations, the brick-wall 2-qubit passes (:679-728, :819-824)."""
 
     def __init__(self, num_qubits, k, optimize_every=5, buffer_factor=2, truncate_every=1,
                  max_nnz_factor=8, use_2qubit_rotations=False, verbose=False, use_fast_eigh=True,
                  use_diag_gate=True, use_kron_cache=True, pr_opt_threshold=0.90, trace=None,
                  pr_tie_tol=1e-12):
-        if use_2qubit_rotations:
-            raise NotImplementedError("oracle restates the 1-qubit passes only")
+        self.use_2qubit_rotations = use_2qubit_rotations
         self.N = num_qubits
         self.k = k
         self.optimize_every = optimize_every
@@ -481,8 +503,36 @@ class OracleBASS:
                         self.trace.accept(j)
             if not improved:
                 break
+        if self.use_2qubit_rotations and self.N >= 2:
+            self._optimize_2q_pass(st, [(i, i + 1) for i in range(0, self.N - 1, 2)])
+            self._optimize_2q_pass(st, [(i, i + 1) for i in range(1, self.N - 1, 2)])
         self._truncate_state(st)
         self._renorm(st)
+
+    # bass_simulator.py:679-728
+    def _optimize_2q_pass(self, st, pairs):
+        for q1, q2 in pairs:
+            rho = rdm_2q(st.x, st.alpha, q1, q2)
+            evals, evecs = np.linalg.eigh(rho)
+            V = evecs[:, np.argsort(-evals)]
+            V_rot = V.conj().T
+            x_save, a_save = st.x, st.alpha
+            pr_before = self._pr(st)
+            st.x, st.alpha = rotate_2q(st.x, st.alpha, q1, q2, V_rot)
+            self._truncate_state(st)
+            frac1 = sum_p(st.alpha)
+            self._renorm(st)
+            st.x, st.alpha = rotate_2q(st.x, st.alpha, q1, q2, V)
+            self._truncate_state(st)
+            frac2 = sum_p(st.alpha)
+            self._renorm(st)
+            pr_after = self._pr(st)
+            # the reference restores when `pr_after > pr_before`; here PR must
+            # drop by more than pr_tie_tol (relative), as for the 1-qubit steps
+            if pr_after > pr_before * (1.0 - self.pr_tie_tol):
+                st.x, st.alpha = x_save, a_save
+            else:
+                self._gamma_running *= np.sqrt(frac1 * frac2)
 
     # bass_simulator.py:829-845
     def optimize_trigger(self, st):

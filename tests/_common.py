@@ -8,6 +8,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 BASS_CASES = ["bass_tfim_n10_k32", "bass_brick_n12_k64", "bass_brick_n16_k256_opt1",
               "bass_haar2q_n12_k128", "bass_brick_n20_k512_trunc2"]
 LARGE_CASES = ["config1_tfim_n24_k65536", "config2_brick_n40_d30_k1024", "config2_brick_n40_d12_k4096"]
+BASS2Q_CASES = ["bass2q_brick_n10_k32", "bass2q_tfim_n10_k48"]   # use_2qubit_rotations=True
 
 
 class Gate:

@@ -131,7 +131,9 @@ def tie_patched_bass(R):
       * ``np.argpartition(probs, -self.k)[-self.k :]`` (simulate, _truncate_state)
         becomes a selection by (|a|^2 descending, key ascending);
       * ``if pr_new >= pr:`` (_optimize_basis) becomes
-        ``if pr_new >= pr * (1.0 - PR_TIE_TOL):``.
+        ``if pr_new >= pr * (1.0 - PR_TIE_TOL):``, and the 2-qubit pass's
+        ``if pr_after > pr_before:`` becomes
+        ``if pr_after > pr_before * (1.0 - PR_TIE_TOL):``.
     """
     import textwrap
     bs = R["bs"]
@@ -143,6 +145,7 @@ def tie_patched_bass(R):
         "simulate": [("np.argpartition(probs, -self.k)[-self.k :]", "_topk_tiebreak(probs, state.x[: state.nnz], self.k)")],
         "_truncate_state": [("np.argpartition(probs, -self.k)[-self.k :]", "_topk_tiebreak(probs, state.x[: state.nnz], self.k)")],
         "_optimize_basis": [("if pr_new >= pr:", "if pr_new >= pr * (1.0 - PR_TIE_TOL):")],
+        "_optimize_2q_pass": [("if pr_after > pr_before:", "if pr_after > pr_before * (1.0 - PR_TIE_TOL):")],
     }
     for name, reps in subs.items():
         src = textwrap.dedent(inspect.getsource(getattr(bs.BASS, name)))
@@ -277,6 +280,54 @@ def kernel_vectors(R, rng):
     return out
 
 
+def kernel_vectors_2q(R, rng):
+    """Known-answer vectors of the 2-qubit RDM and 2-qubit rotation kernels."""
+    bs = R["bs"]
+    out = {}
+    N, n = 12, 300
+    x = np.unique(rng.integers(0, 2 ** N, size=2 * n).astype(np.uint64))[:n]
+    rng.shuffle(x)
+    a = rng.standard_normal(len(x)) + 1j * rng.standard_normal(len(x))
+    a /= np.linalg.norm(a)
+    out["x"] = x; out["a"] = a
+    for (q1, q2) in ((0, 1), (3, 7), (11, 4)):
+        rho = bs.compute_2qubit_rdm(x, a, len(x), q1, q2)
+        evals, evecs = np.linalg.eigh(rho)
+        V = evecs[:, np.argsort(-evals)]
+        U4 = np.ascontiguousarray(V.conj().T)
+        x2 = np.concatenate([x, np.zeros(3 * len(x), np.uint64)])
+        a2 = np.concatenate([a, np.zeros(3 * len(x), np.complex128)])
+        m = bs.apply_2qubit_rotation_sparse(x2, a2, len(x), q1, q2, U4)
+        o = np.argsort(x2[:m])
+        out[f"rdm2q_{q1}_{q2}"] = rho
+        out[f"rot2q_{q1}_{q2}_U"] = U4
+        out[f"rot2q_{q1}_{q2}_x"] = x2[:m][o].copy(); out[f"rot2q_{q1}_{q2}_a"] = a2[:m][o].copy()
+    return out
+
+
+def main_2q(R, pkg):
+    """The 2-qubit rotation fixtures only (kernels2q.npz and the bass2q runs)."""
+    rng = np.random.default_rng(20261204)
+    kv = kernel_vectors_2q(R, rng)
+    np.savez_compressed(os.path.join(HERE, "kernels2q.npz"), **kv)
+    print("kernels2q.npz", len(kv))
+    cases = [
+        ("bass2q_brick_n10_k32", 10, 32, pkg.circuits.brickwork_circuit(10, 8, rng=np.random.default_rng(21)),
+         {"use_2qubit_rotations": True}),
+        ("bass2q_tfim_n10_k48", 10, 48, pkg.circuits.tfim_circuit(
+            10, 10, J=1.0, h=1.0, dt=0.3, rng=np.random.default_rng(22), disorder_strength_h=0.5),
+         {"use_2qubit_rotations": True}),
+    ]
+    for name, N, k, circ, kw in cases:
+        r = run_bass(R, N, k, circ, patched=True, **kw)
+        meta, mats = gate_arrays(circ)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), N=np.int64(N), k=np.int64(k),
+                            kwargs=np.array(repr(kw)), gate_meta=meta, gate_mats=mats,
+                            pr_tie_tol=np.float64(PR_TIE_TOL), **r)
+        print(name, "events", len(r["events"]), "nnz", len(r["x"]), "gamma", float(r["gamma"]),
+              "min_gap", float(r["min_gap"]), f"{float(r['seconds']):.2f}s")
+
+
 def oracle_free_haar(rng):
     z = (rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))) / np.sqrt(2.0)
     q, r = np.linalg.qr(z)
@@ -288,10 +339,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--skip-large", action="store_true")
+    ap.add_argument("--only-2q", action="store_true", help="write only the 2-qubit rotation fixtures")
     args = ap.parse_args()
     oracle.build()
     R = import_reference(args.reference)
     pkg = load_pkg()
+    if args.only_2q:
+        main_2q(R, pkg)
+        return
     rng = np.random.default_rng(20261203)
 
     # kernel-level known-answer vectors
