@@ -95,6 +95,7 @@ def load_library():
         "bass_ctrl_init": (I32, [P, P, I64, D, P]),
         "bass_gate_1q": (I32, [P, P, P, I32, Trunc, P, P, SZ, P]),
         "bass_gate_2q": (I32, [P, P, P, P, I32, I32, Trunc, P, P, SZ, P]),
+        "bass_rotate_2q": (I32, [P, P, P, P, I32, I32, Trunc, P, P, SZ, P]),
         "bass_phase_1q": (I32, [P, P, P, I32, P, P, SZ, P]),
         "bass_phase_2q": (I32, [P, P, I32, I32, P, P]),
         "bass_topk": (I32, [P, P, Trunc, P, P, SZ, P]),
@@ -104,6 +105,7 @@ def load_library():
         "bass_pr": (I32, [P, P, P, SZ, P]),
         "bass_norm2": (I32, [P, P, P, SZ, P]),
         "bass_rdm_1q": (I32, [P, I32, P, P, P, SZ, P]),
+        "bass_rdm_2q": (I32, [P, P, I32, I32, P, P, P, SZ, P]),
         "bass_rotate_step": (I32, [P, P, P, I32, I64, I32, P, P, SZ, P]),
         "bass_fingerprint": (I32, [P, D, P, P, SZ, P]),
         "bass_radix_sort_u64": (I32, [P, P, I64, I32, P, SZ, P, P]),

@@ -32,8 +32,6 @@ class BASS:
                  use_2qubit_rotations=False, verbose=False, use_fast_eigh=True, use_diag_gate=True,
                  use_kron_cache=True, pr_opt_threshold=0.90, *, pr_tie_tol=1e-12, trace=False,
                  trace_cap=None):
-        if use_2qubit_rotations:
-            raise NotImplementedError("use_2qubit_rotations=True is not supported by the GPU path")
         self.N = num_qubits
         self.k = k
         self.optimize_every = optimize_every
@@ -114,8 +112,40 @@ class BASS:
                         self.stats["accepted"] += 1
             if not improved:
                 break
+        if self.use_2qubit_rotations and self.N >= 2:     # bass_simulator.py:819-824
+            self._optimize_2q_pass(state, [(i, i + 1) for i in range(0, self.N - 1, 2)])
+            self._optimize_2q_pass(state, [(i, i + 1) for i in range(1, self.N - 1, 2)])
         state._topk(nat.trunc(self.k, self.k))   # _truncate_state
         state._renorm(int(self.trace))           # _renorm
+
+    # bass_simulator.py:679-728
+    def _optimize_2q_pass(self, state, pairs):
+        """Brick-wall 2-qubit truncation alignment: per pair, rotate into the
+        eigenbasis of its 4x4 RDM, truncate, rotate back, truncate; keep the
+        result if PR drops by more than pr_tie_tol (relative; the reference
+        keeps it unless PR rose), with gamma *= sqrt(frac1 * frac2)."""
+        eng = state._eng
+        tr = nat.trunc(self.k, self.k)             # _truncate_state, fused into each rotation
+        for q1, q2 in pairs:
+            rho = state._rdm_2q(q1, q2)
+            evals, evecs = np.linalg.eigh(rho)
+            V = evecs[:, np.argsort(-evals)]
+            pr_before = state._pr()
+            state._rotate_2q(V.conj().T, q1, q2, tr)
+            spare = state._spare()
+            nat.swap(state._tmp2, spare)           # the saved state, until the decision
+            frac1 = state._norm2()
+            state._renorm(int(self.trace))
+            state._rotate_2q(V, q1, q2, tr)
+            frac2 = state._norm2()
+            state._renorm(int(self.trace))
+            pr_after = state._pr()
+            if pr_after > pr_before * (1.0 - self.pr_tie_tol):
+                nat.swap(state._cur, spare)        # restore
+                state._touch()
+            else:
+                g = float(eng.read_ctrl()["gamma_running"])
+                eng.set_ctrl("gamma_running", g * np.sqrt(frac1 * frac2))
 
     def _general_truncation(self, state, hard_cap, gates_since):
         """The simulate-level truncation rule when truncate_every > 1 (host decides)."""

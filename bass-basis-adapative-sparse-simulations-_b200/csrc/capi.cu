@@ -253,6 +253,38 @@ int bass_gate_2q(const bass_state* in, bass_state* tmp, bass_state* out, const d
   return status_of(e);
 }
 
+int bass_rotate_2q(const bass_state* in, bass_state* tmp, bass_state* out, const double* host_U4, int q1,
+                   int q2, bass_trunc tr, bass_ctrl* ctrl, void* ws, size_t ws_bytes, void* stream) {
+  if (!in || !tmp || !out || in == tmp || tmp == out || in == out || !host_U4 || q1 < 0 || q2 < 0 ||
+      q1 >= BASS_MAX_QUBITS || q2 >= BASS_MAX_QUBITS || q1 == q2 || !ctrl)
+    return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  cudaStream_t s = (cudaStream_t)stream;
+  // pass 1: bring q2 to the lowest physical bit (a pure reorder)
+  OpArgs a{};
+  a.in = in; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = q2; a.gb = 0;
+  bass_trunc none{};
+  none.k_cond = -1;
+  cudaError_t e = run_merge_op(K_PERM, a, none, 0, 0, s);
+  if (e != cudaSuccess) return status_of(e);
+  // pass 2: groups of four (b_q1, b_q2), the rotation's drop rule
+  OpArgs b{};
+  b.in = tmp; b.out = out; b.ctrl = ctrl; b.ws = v; b.q = q1; b.gb = 1; b.drop_zero = 2;
+  load_G(b, host_U4, 16);
+  e = run_merge_op(K_GATE2, b, tr, 0, 0, s);
+  if (e == cudaSuccess && tr.trace) e = run_fingerprint(out, kSigPmin, nullptr, v, s, ctrl, 1, 1);
+  return status_of(e);
+}
+
+int bass_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* rho, bass_ctrl* ctrl, void* ws,
+                size_t ws_bytes, void* stream) {
+  if (!st || !tmp || st == tmp || !rho || !ctrl || q1 < 0 || q2 < 0 || q1 >= BASS_MAX_QUBITS ||
+      q2 >= BASS_MAX_QUBITS || q1 == q2)
+    return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  return status_of(run_rdm_2q(st, tmp, q1, q2, rho, ctrl, v, (cudaStream_t)stream));
+}
+
 int bass_phase_1q(bass_state* st, bass_state* tmp, const double* host_diag2, int q, bass_ctrl* ctrl,
                   void* ws, size_t ws_bytes, void* stream) {
   if (!st || !tmp || st == tmp || !host_diag2 || q < 0 || q >= BASS_MAX_QUBITS || !ctrl) return BASS_ERR_ARG;

@@ -264,7 +264,9 @@ __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t*
         have = true;
       }
       ca[o] = acc;
-      if (have) mask |= 1u << o;
+      // drop_zero 2 (a 2-qubit rotation): the rotation's rule |a| > 1e-30
+      // (bass_simulator.py:275) instead of "some product was non-zero"
+      if (drop_zero == 2 ? above_drop(acc) : have) mask |= 1u << o;
     }
   } else if (KIND == K_ROT1) {
     const double2 zero = make_double2(0.0, 0.0);
@@ -472,7 +474,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
   if (bad && blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
   if (bad && PASS != P_WRITE) return;
   const bool scaled = !(H.r0 == 1.0 && H.r1 == 1.0);
-  const long long nitems = (bad || skip) ? 0 : (KIND == K_RDM) ? ntiles * a.nsets : ntiles;
+  // P_RDM: items are (set, tile); K_RDM sets are qubits, the 4x4 moments of
+  // a qubit pair (K_GATE2) split into a.nsets = 4 sets of four values that
+  // share one partition
+  const long long nitems = (bad || skip) ? 0 : (PASS == P_RDM) ? ntiles * a.nsets : ntiles;
   long long cnt = 0;
   const int base_e = tid * kPerThread;
 
@@ -481,9 +486,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
     __syncthreads();
     const long long item = sItem;
     if (item >= nitems) break;
-    const int set = (KIND == K_RDM) ? (int)(item / ntiles) : 0;
-    const long long tile = (KIND == K_RDM) ? item % ntiles : item;
+    const int set = (PASS == P_RDM) ? (int)(item / ntiles) : 0;
+    const long long tile = (PASS == P_RDM) ? item % ntiles : item;
     const int t = (KIND == K_RDM) ? a.in->pos[a.q + set] : H.t;
+    const int pset = (KIND == K_RDM) ? set : 0;  // the partition records this item reads
 
     // ---- segments ---------------------------------------------------------
     if (tid == 0) {
@@ -494,7 +500,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
         len[0] = (H.n - lo[0] < kTile) ? H.n - lo[0] : kTile;
         zs = lo[0];
       } else {
-        const long long* rc = a.ws.part + ((long long)set * (a.ws.max_tiles + 1) + tile) * 6;
+        const long long* rc = a.ws.part + ((long long)pset * (a.ws.max_tiles + 1) + tile) * 6;
         const long long* rn = rc + 6;
         zs = rc[0];
         if (rc[1] == rn[1]) {
@@ -639,7 +645,55 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
     // ---- evaluate ------------------------------------------------------------
     // Round r gives position r * kThreads + tid to thread tid, so neighbouring
     // threads handle neighbouring groups and write neighbouring outputs.
-    if (PASS == P_RDM) {
+    if (PASS == P_RDM && KIND == K_GATE2) {
+      // 4x4 moments of the pair (q1 at bit 1, q2 at bit 0 after the first
+      // pass): per group of up to four entries a_i (i = (b_q1 << 1) | b_q2),
+      // set 0: |a_0|^2 .. |a_3|^2; set 1: Re/Im a_0 conj(a_1), a_0 conj(a_2);
+      // set 2: a_0 conj(a_3), a_1 conj(a_2); set 3: a_1 conj(a_3), a_2 conj(a_3)
+      // (bass_simulator.py:200-231, rho[p][q] += a_p conj(a_q)).
+      i128 v[4] = {0, 0, 0, 0};
+      double dh[4] = {0.0, 0.0, 0.0, 0.0}, dl[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int p = tid; p < E; p += kThreads) {
+        const uint64_t gid = sZ[p] >> 2;
+        if (p > 0 && (sZ[p - 1] >> 2) == gid) continue;
+        const double2 zero = make_double2(0.0, 0.0);
+        double2 g0 = zero, g1 = zero, g2 = zero, g3 = zero;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          if (p + r < E) {
+            const uint64_t zr = sZ[p + r];
+            if ((zr >> 2) == gid) {
+              const double2 v2 = amp(p + r);
+              const unsigned i = (unsigned)(zr & 3);
+              if (i == 0) g0 = v2;
+              else if (i == 1) g1 = v2;
+              else if (i == 2) g2 = v2;
+              else g3 = v2;
+            }
+          }
+        }
+        double m[4];
+        if (set == 0) {
+          m[0] = prob(g0); m[1] = prob(g1); m[2] = prob(g2); m[3] = prob(g3);
+        } else {
+          // the set's two pairs (i, j), i < j: a_i conj(a_j)
+          const double2 ai = set == 3 ? g1 : g0, aj = set == 1 ? g1 : g3;
+          const double2 bi = set == 1 ? g0 : set == 2 ? g1 : g2, bj = set == 3 ? g3 : g2;
+          const double2 c0 = cmul(ai, make_double2(aj.x, -aj.y));
+          const double2 c1 = cmul(bi, make_double2(bj.x, -bj.y));
+          m[0] = c0.x; m[1] = c0.y; m[2] = c1.x; m[3] = c1.y;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) fx_acc96(m[k], dh[k], dl[k], v[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] += fx_join96s(dh[k], dl[k]);
+      block_sum_i128<4>(v, sRed);
+      if (tid == 0) {
+        Partial* pt = a.ws.partials + (long long)set * a.ws.max_tiles + tile;
+        pt->s[0] = v[0]; pt->s[1] = v[1]; pt->s[2] = v[2]; pt->s[3] = v[3];
+      }
+    } else if (PASS == P_RDM) {
       // at most kPerThread positions per thread, so at most eight terms per
       // split accumulator (fx_acc96) before they are joined
       i128 v[4] = {0, 0, 0, 0};
@@ -1820,6 +1874,27 @@ cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, 
   KLAUNCH(S_PARTITION, s, launch_pdl(k_partition, dim3(device().grid_small, nq), dim3(256), 0, s, a, (int)K_RDM, 1));
   if ((e = launch_tile<K_RDM, P_RDM>(a, 0, s, nullptr)) != cudaSuccess) return e;
   KLAUNCH(S_RDM_FINAL, s, k_rdm_final<<<nq, 256, 0, s>>>(st, rho, ws, 0));
+  return cudaGetLastError();
+}
+
+// 4x4 moments of the qubit pair (q1, q2): the first pass of a 2-qubit gate
+// brings q2 to bit 0 (st -> tmp), then one moment pass over tmp groups the
+// entries by every other bit with q1 at bit 1.  rho: 16 doubles, see k_tile's
+// P_RDM pass for K_GATE2 (set s writes rho[4 s .. 4 s + 3]).
+cudaError_t run_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* rho, bass_ctrl* ctrl,
+                       const WsView& ws, cudaStream_t s) {
+  OpArgs a{};
+  a.in = st; a.out = tmp; a.ctrl = ctrl; a.ws = ws; a.q = q2; a.gb = 0;
+  bass_trunc none{};
+  none.k_cond = -1;
+  cudaError_t e = run_merge_op(K_PERM, a, none, 0, 0, s);
+  if (e != cudaSuccess) return e;
+  OpArgs b{};
+  b.in = tmp; b.out = nullptr; b.ctrl = ctrl; b.ws = ws; b.q = q1; b.gb = 1; b.nsets = 4;
+  // the partition also clears the small workspace region
+  KLAUNCH(S_PARTITION, s, launch_pdl(k_partition, dim3(device().grid_small, 1), dim3(256), 0, s, b, (int)K_GATE2, 1));
+  if ((e = launch_tile<K_GATE2, P_RDM>(b, 0, s, nullptr)) != cudaSuccess) return e;
+  KLAUNCH(S_RDM_FINAL, s, k_rdm_final<<<4, 256, 0, s>>>(tmp, rho, ws, 0));
   return cudaGetLastError();
 }
 

@@ -124,6 +124,39 @@ class SparseState:
         nat.swap(self._cur, self._tmp2)
         self._touch()
 
+    def _rotate_2q(self, U4, q1, q2, tr):
+        """bass_simulator.py:237-289 apply_2qubit_rotation_sparse with the
+        truncation tr fused; the previous state is left in _tmp2."""
+        eng = self._eng
+        u = nat.host_c128(U4)
+        nat.check(eng.L.bass_rotate_2q(self._cur.ptr, self._tmp.ptr, self._tmp2.ptr, nat._host(u), int(q1),
+                                       int(q2), tr, eng.ctrl_ptr, eng.ws_ptr, eng.ws_bytes, eng.stream),
+                  "bass_rotate_2q")
+        nat.swap(self._cur, self._tmp2)
+        self._touch()
+
+    def _rdm_2q(self, q1, q2) -> np.ndarray:
+        """bass_simulator.py:200-231 compute_2qubit_rdm: 4x4 complex, index
+        (bit_q1 << 1) | bit_q2 (synchronising)."""
+        eng = self._eng
+        nat.check(eng.L.bass_rdm_2q(self._cur.ptr, self._tmp.ptr, int(q1), int(q2),
+                                    nat.ctypes.c_void_p(nat._ptr(eng.rho)), eng.ctrl_ptr, eng.ws_ptr,
+                                    eng.ws_bytes, eng.stream), "bass_rdm_2q")
+        r = eng.rho[:16].cpu().numpy()
+        rho = np.zeros((4, 4), dtype=np.complex128)
+        for i in range(4):
+            rho[i, i] = r[i]
+        for n, (i, j) in enumerate([(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]):
+            rho[i, j] = complex(r[4 + 2 * n], r[5 + 2 * n])
+            rho[j, i] = np.conj(rho[i, j])
+        return rho
+
+    def _spare(self):
+        """A fourth device buffer (the 2-qubit passes park the saved state there)."""
+        if getattr(self, "_tmp3", None) is None:
+            self._tmp3 = nat.DevState(self._eng, self._cur.cap)
+        return self._tmp3
+
     def _phase_2q(self, diag, q1, q2):
         eng = self._eng
         d = nat.host_c128(diag)

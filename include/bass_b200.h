@@ -157,6 +157,14 @@ int bass_gate_1q(const bass_state* in, bass_state* out, const double* host_G, in
 int bass_gate_2q(const bass_state* in, bass_state* tmp, bass_state* out, const double* host_G,
                  int q1, int q2, bass_trunc tr, bass_ctrl* ctrl, void* ws, size_t ws_bytes,
                  void* stream);
+/* 2-qubit basis rotation: bass_simulator.py:237-289
+   apply_2qubit_rotation_sparse (used by the brick-wall pair passes,
+   :679-728) + optional truncation.  As bass_gate_2q, but a child is kept when
+   |a| > 1e-30 (the rotation's drop rule).  U4: 4x4 complex128, index
+   (bit_q1 << 1) | bit_q2, host pointer.  Output key-sorted. */
+int bass_rotate_2q(const bass_state* in, bass_state* tmp, bass_state* out, const double* host_U4,
+                   int q1, int q2, bass_trunc tr, bass_ctrl* ctrl, void* ws, size_t ws_bytes,
+                   void* stream);
 /* Diagonal 1-qubit gate in place (g01 = g10 = 0): children of the reference's
    1-qubit kernel that are exactly zero are dropped (compacts only if one is). */
 int bass_phase_1q(bass_state* st, bass_state* tmp, const double* host_diag2, int q, bass_ctrl* ctrl,
@@ -191,6 +199,13 @@ int bass_norm2(const bass_state* st, double* out, void* ws, size_t ws_bytes, voi
    (rho00, rho11, Re rho01, Im rho01), device doubles. */
 int bass_rdm_1q(const bass_state* st, int num_qubits, double* rho, bass_ctrl* ctrl, void* ws,
                 size_t ws_bytes, void* stream);
+/* bass_simulator.py:200-231 compute_2qubit_rdm for the qubit pair (q1, q2),
+   index (bit_q1 << 1) | bit_q2, rho[p][q] = sum over groups of a_p conj(a_q),
+   exact sums.  rho: 16 device doubles, (rho00, rho11, rho22, rho33,
+   Re/Im rho01, Re/Im rho02, Re/Im rho03, Re/Im rho12, Re/Im rho13,
+   Re/Im rho23); the lower triangle is the conjugate.  tmp is scratch. */
+int bass_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* rho, bass_ctrl* ctrl,
+                void* ws, size_t ws_bytes, void* stream);
 /* bass_rdm_1q for callers that cannot allocate device memory (a stream being
    captured into a CUDA graph, a host runtime that owns all device memory, an
    embedding that may only pass the buffers it was given).  No counterpart in
