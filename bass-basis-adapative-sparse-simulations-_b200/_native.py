@@ -106,6 +106,9 @@ def load_library():
         "bass_norm2": (I32, [P, P, P, SZ, P]),
         "bass_rdm_1q": (I32, [P, I32, P, P, P, SZ, P]),
         "bass_rdm_2q": (I32, [P, P, I32, I32, P, P, P, SZ, P]),
+        "bass_to_dense": (I32, [P, P, I32, P, P, P]),
+        "bass_dense_dot": (I32, [P, P, I64, P, P, P, SZ, P]),
+        "bass_sparse_dot": (I32, [P, P, I32, P, P, P, SZ, P]),
         "bass_rotate_step": (I32, [P, P, P, I32, I64, I32, P, P, SZ, P]),
         "bass_fingerprint": (I32, [P, D, P, P, SZ, P]),
         "bass_radix_sort_u64": (I32, [P, P, I64, I32, P, SZ, P, P]),

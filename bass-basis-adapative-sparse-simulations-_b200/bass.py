@@ -233,6 +233,10 @@ class BASS:
             psi = np.einsum("ij,kjl->kil", self.U[j], psi3d).reshape(-1)
         return psi
 
+    def to_statevector_device(self, state):
+        """to_statevector on the device (torch complex128), for N <= 30."""
+        return state.to_dense_device(U=self.U)
+
     def trace_events(self):
         """The device trace of the last simulate() call (trace=True)."""
         if self.last_state is None:

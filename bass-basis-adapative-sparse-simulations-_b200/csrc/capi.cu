@@ -285,6 +285,25 @@ int bass_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* r
   return status_of(run_rdm_2q(st, tmp, q1, q2, rho, ctrl, v, (cudaStream_t)stream));
 }
 
+int bass_to_dense(const bass_state* st, const double* host_U, int nq, double* psi, bass_ctrl* ctrl, void* stream) {
+  if (!st || !psi || !ctrl || nq < 1 || nq > 30) return BASS_ERR_ARG;
+  return status_of(run_to_dense(st, host_U, nq, psi, ctrl, (cudaStream_t)stream));
+}
+
+int bass_dense_dot(const double* u, const double* v, int64_t n, double* out, bass_ctrl* ctrl, void* ws,
+                   size_t ws_bytes, void* stream) {
+  if (!u || !v || !out || !ctrl || n < 0) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, w);
+  return status_of(run_dot(u, v, n, nullptr, 64, out, ctrl, w, (cudaStream_t)stream));
+}
+
+int bass_sparse_dot(const bass_state* st, const double* psi, int nq, double* out, bass_ctrl* ctrl, void* ws,
+                    size_t ws_bytes, void* stream) {
+  if (!st || !psi || !out || !ctrl || nq < 1 || nq > 30) return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, w);
+  return status_of(run_dot(psi, nullptr, 0, st, nq, out, ctrl, w, (cudaStream_t)stream));
+}
+
 int bass_phase_1q(bass_state* st, bass_state* tmp, const double* host_diag2, int q, bass_ctrl* ctrl,
                   void* ws, size_t ws_bytes, void* stream) {
   if (!st || !tmp || st == tmp || !host_diag2 || q < 0 || q >= BASS_MAX_QUBITS || !ctrl) return BASS_ERR_ARG;

@@ -95,6 +95,10 @@ cudaError_t run_merge_op(int kind, OpArgs a, const bass_trunc& tr, int finalize_
 cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
                     cudaStream_t s);
 cudaError_t zero_small(const WsView& ws, cudaStream_t s);
+cudaError_t run_to_dense(const bass_state* st, const double* host_U, int nq, double* psi, bass_ctrl* ctrl,
+                         cudaStream_t s);
+cudaError_t run_dot(const double* u, const double* v, long long n, const bass_state* st, int nq, double* out,
+                    bass_ctrl* ctrl, const WsView& ws, cudaStream_t s);
 cudaError_t run_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* rho, bass_ctrl* ctrl,
                        const WsView& ws, cudaStream_t s);
 cudaError_t run_rdm_prepared(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,

@@ -552,6 +552,142 @@ __global__ void k_merge_out(uint64_t* keys, double2* amps, WsView ws, long long*
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// dense vectors (bass_simulator.py:608-621 to_statevector; fidelity.py:48-68
+// compute_fidelity, runner.py:620-626 np.vdot), for n <= 30 qubits
+// ---------------------------------------------------------------------------
+// psi[true key] = a (pending scale applied); psi was zeroed.  A key with a
+// bit at or above nq (a state of more qubits than psi holds) is refused.
+__global__ void k_dense_scatter(const bass_state* st, double2* psi, int nq, bass_ctrl* c) {
+  __shared__ int8_t qat[64];
+  if (threadIdx.x < 64) qat[threadIdx.x] = st->qat[threadIdx.x];
+  __syncthreads();
+  const long long n = st->nnz;
+  const double r0 = st->rscale[0], r1 = st->rscale[1];
+  const double2* amps = reinterpret_cast<const double2*>(st->amps);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+  {
+    const uint64_t tk = true_key(st->keys[i], qat, 64);
+    if (tk >> nq) {
+      set_error(c, BASS_ERR_ARG);
+      continue;
+    }
+    psi[tk] = scale_load(amps[i], r0, r1);
+  }
+}
+
+// U applied to qubit j of a dense vector of 2 half entries: each pair
+// (bit j clear, bit j set) becomes (u00 a0 + u01 a1, u10 a0 + u11 a1).
+__global__ void k_dense_1q(double2* psi, long long half, int j, double2 u00, double2 u01, double2 u10,
+                           double2 u11) {
+  const long long lowmask = (1LL << j) - 1;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < half;
+       p += (long long)gridDim.x * blockDim.x) {
+    const long long i0 = ((p & ~lowmask) << 1) | (p & lowmask), i1 = i0 | (1LL << j);
+    const double2 a0 = psi[i0], a1 = psi[i1];
+    psi[i0] = cadd(cmul(u00, a0), cmul(u01, a1));
+    psi[i1] = cadd(cmul(u10, a0), cmul(u11, a1));
+  }
+}
+
+// Per-CTA exact partial sums of conj(u_i) v_i (re, im) into ws.red[2 b ..];
+// sparse: u is psi at the state's true keys and v its amplitudes.
+template <bool SPARSE>
+__global__ void __launch_bounds__(256) k_dot(const double2* u, const double2* v, long long n,
+                                             const bass_state* st, int nq, WsView ws, bass_ctrl* ctl) {
+  __shared__ i128 sRed[2 * 8];
+  __shared__ int8_t qat[64];
+  long long nn = n;
+  double r0 = 1.0, r1 = 1.0;
+  const double2* amps = v;
+  if (SPARSE) {
+    if (threadIdx.x < 64) qat[threadIdx.x] = st->qat[threadIdx.x];
+    __syncthreads();
+    nn = st->nnz;
+    r0 = st->rscale[0];
+    r1 = st->rscale[1];
+    amps = reinterpret_cast<const double2*>(st->amps);
+  }
+  i128 acc[2] = {0, 0};
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < nn; i0 += 8 * stride) {
+    double h[2] = {0.0, 0.0}, l[2] = {0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const long long i = i0 + k * stride;
+      if (i >= nn) break;
+      double2 a, b;
+      if (SPARSE) {
+        const uint64_t tk = true_key(st->keys[i], qat, 64);
+        if (tk >> nq) {  // refused as in k_dense_scatter
+          set_error(ctl, BASS_ERR_ARG);
+          continue;
+        }
+        a = u[tk];
+        b = scale_load(amps[i], r0, r1);
+      } else {
+        a = u[i];
+        b = v[i];
+      }
+      const double2 c = cmul(make_double2(a.x, -a.y), b);
+      fx_acc96(c.x, h[0], l[0], acc[0]);
+      fx_acc96(c.y, h[1], l[1], acc[1]);
+    }
+    acc[0] += fx_join96s(h[0], l[0]);
+    acc[1] += fx_join96s(h[1], l[1]);
+  }
+  block_sum_i128<2>(acc, sRed);
+  if (threadIdx.x == 0) {
+    ws.red[2 * blockIdx.x] = acc[0];
+    ws.red[2 * blockIdx.x + 1] = acc[1];
+  }
+}
+
+__global__ void k_dot_final(WsView ws, int nblk, double* out) {
+  __shared__ i128 sRed[2 * 8];
+  i128 acc[2] = {0, 0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    acc[0] += ws.red[2 * b];
+    acc[1] += ws.red[2 * b + 1];
+  }
+  block_sum_i128<2>(acc, sRed);
+  if (threadIdx.x == 0) {
+    out[0] = fx_to(acc[0]);
+    out[1] = fx_to(acc[1]);
+  }
+}
+
+cudaError_t run_to_dense(const bass_state* st, const double* host_U, int nq, double* psi, bass_ctrl* ctrl,
+                         cudaStream_t s) {
+  const long long n = 1LL << nq;
+  cudaError_t e = cudaMemsetAsync(psi, 0, (size_t)n * 16, s);
+  if (e != cudaSuccess) return e;
+  double2* p = reinterpret_cast<double2*>(psi);
+  KLAUNCH(S_SMALL, s, k_dense_scatter<<<device().grid_small, 256, 0, s>>>(st, p, nq, ctrl));
+  if (host_U) {
+    const int grid = device().sms * 8;
+    for (int j = 0; j < nq; ++j) {
+      const double* u = host_U + 8 * j;
+      KLAUNCH(S_SMALL, s,
+              k_dense_1q<<<grid, 256, 0, s>>>(p, n / 2, j, make_double2(u[0], u[1]), make_double2(u[2], u[3]),
+                                               make_double2(u[4], u[5]), make_double2(u[6], u[7])));
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t run_dot(const double* u, const double* v, long long n, const bass_state* st, int nq, double* out,
+                    bass_ctrl* ctrl, const WsView& ws, cudaStream_t s) {
+  const int grid = 512;  // ws.red holds 1024 partials: two per CTA
+  const double2* a = reinterpret_cast<const double2*>(u);
+  const double2* b = reinterpret_cast<const double2*>(v);
+  if (st) KLAUNCH(S_REDUCE, s, k_dot<true><<<grid, 256, 0, s>>>(a, b, 0, st, nq, ws, ctrl));
+  else KLAUNCH(S_REDUCE, s, k_dot<false><<<grid, 256, 0, s>>>(a, b, n, nullptr, 64, ws, ctrl));
+  KLAUNCH(S_REDUCE, s, k_dot_final<<<1, 256, 0, s>>>(ws, grid, out));
+  return cudaGetLastError();
+}
+
 cudaError_t run_reduce(const bass_state* st, int mode, double* dest, bass_ctrl* ctrl,
                        const WsView& ws, cudaStream_t s) {
   const int grid = device().grid_small > 1024 ? 1024 : device().grid_small;

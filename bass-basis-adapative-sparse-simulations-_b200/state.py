@@ -90,6 +90,24 @@ class SparseState:
         dense[x.astype(np.int64)] = a
         return dense
 
+    def to_dense_device(self, U=None):
+        """The dense statevector on the device (torch complex128, 2^N entries,
+        N <= 30): the entries at their true keys, then each frame U[j] applied
+        to qubit j (bass_simulator.py:608-621 with U = the BASS frames)."""
+        eng = self._eng
+        if self.N > 30:
+            raise ValueError(f"N={self.N} too large for a dense statevector")
+        torch = eng.torch
+        psi = torch.empty(2 ** self.N, dtype=torch.complex128, device=eng.device)
+        hu = None
+        if U is not None:
+            hu = nat.host_c128(np.stack([np.asarray(u, dtype=np.complex128) for u in U]))
+        nat.check(eng.L.bass_to_dense(self._cur.ptr, None if hu is None else nat._host(hu), int(self.N),
+                                      nat.ctypes.c_void_p(psi.data_ptr()), eng.ctrl_ptr, eng.stream),
+                  "bass_to_dense")
+        eng.check_errors()
+        return psi
+
     def probability_distribution(self):
         return np.abs(self.alpha) ** 2 / (self.gamma ** 2)
 

@@ -206,6 +206,21 @@ int bass_rdm_1q(const bass_state* st, int num_qubits, double* rho, bass_ctrl* ct
    Re/Im rho23); the lower triangle is the conjugate.  tmp is scratch. */
 int bass_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* rho, bass_ctrl* ctrl,
                 void* ws, size_t ws_bytes, void* stream);
+/* bass_simulator.py:608-621 to_statevector on the device: psi (2^nq
+   complex128, device) = the state at its true keys (pending scale applied),
+   then each frame U_j applied to logical qubit j in order (host_U: nq 2x2
+   complex128 row-major; NULL for no frames).  nq <= 30; a key of more
+   qubits than nq sets BASS_ERR_ARG and is skipped. */
+int bass_to_dense(const bass_state* st, const double* host_U, int nq, double* psi, bass_ctrl* ctrl,
+                  void* stream);
+/* runner.py:620-626 np.vdot(u, v) of two device complex128 vectors of n
+   entries: out[0..1] = sum conj(u_i) v_i, exact sums (device doubles). */
+int bass_dense_dot(const double* u, const double* v, int64_t n, double* out, bass_ctrl* ctrl, void* ws,
+                   size_t ws_bytes, void* stream);
+/* fidelity.py:48-68 compute_fidelity's overlap: out[0..1] = sum over the
+   state's entries of conj(psi[x]) a_x (psi: dense 2^nq complex128, device). */
+int bass_sparse_dot(const bass_state* st, const double* psi, int nq, double* out, bass_ctrl* ctrl, void* ws,
+                    size_t ws_bytes, void* stream);
 /* bass_rdm_1q for callers that cannot allocate device memory (a stream being
    captured into a CUDA graph, a host runtime that owns all device memory, an
    embedding that may only pass the buffers it was given).  No counterpart in
