@@ -64,12 +64,13 @@ typedef struct bass_state {
 
 #define BASS_TRACE_WORDS 7 /* u64 per trace event, see bass_ctrl.trace */
 /* Kernel slots of the profiler: 0..29 are the tile kernels (kind * 5 + pass,
-   kind: 0 gate1, 1 rot1, 2 gate2, 3 perm, 4 plain, 5 rdm; pass: 0 hist,
-   1 hist2, 2 gather, 3 write, 4 rdm), then 30 partition, 31 select1,
-   32 select2, 33 select_exact, 34 finalize, 35 reductions, 36 fingerprint,
-   37 phase2q, 38 phase1q, 39 rdm_final, 40 radix sort, 41 merge runs,
-   42 small bookkeeping kernels, 43 / 44 level-1 / level-2 slot histograms,
-   45 slot gather, 46 tie marking and per-tile survivor counts. */
+   kind: 0 gate1, 1 rot1, 2 gate2, 3 perm, 4 plain, 5 rdm; pass: 0 evaluation,
+   3 write (the compaction for gate, rotation and truncation kinds), 4 moments;
+   passes 1 and 2 are unused), then 30 partition, 31 selection (one launch),
+   35 reductions (norm, PR, dot products, the traced rotation commit),
+   36 fingerprint, 37 phase2q, 38 phase1q, 39 rdm_final, 40 radix sort,
+   41 merge runs, 42 small bookkeeping kernels (dense statevectors among
+   them).  Slots 32-34 and 43-47 are unused and keep the numbering stable. */
 #define BASS_PROF_SLOTS 48
 
 typedef struct bass_ctrl {
