@@ -20,6 +20,7 @@ def _make_golden():
 
 
 @pytest.mark.skipif(not os.path.isdir(REF), reason="the reference sources are not on this machine")
+@pytest.mark.filterwarnings("ignore::SyntaxWarning")   # a docstring escape in the reference's runner
 def test_reference_runner_uses_gpu_classes(pkg):
     mg = _make_golden()
     before = {k: v for k, v in sys.modules.items() if k == "src" or k.startswith("src.")}
