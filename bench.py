@@ -203,15 +203,7 @@ def run_ours(a, rank, world, dist):
         ups.append(b.stats["amp_updates"])
     launches = (L.bass_launch_count() - launches0) // max(a.steps, 1)
     clocks = sampler.stop()
-    t_total = sum(times)
-    if dist is not None:
-        tt = torch.tensor([t_total], dtype=torch.float64, device=dev)
-        uu = torch.tensor([float(sum(ups))], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dist.all_reduce(uu, op=dist.ReduceOp.SUM)
-        t_total, u_total = float(tt.item()), float(uu.item())
-    else:
-        u_total = float(sum(ups))
+    t_total, u_total = over_ranks(dist, dev, sum(times), float(sum(ups)))
     value = u_total / t_total
 
     # end to end through the public API: host circuit in, host state (x, alpha) out
@@ -229,16 +221,8 @@ def run_ours(a, rank, world, dist):
         e2e_u.append(b.stats["amp_updates"])
         h2d = sum(g.matrix.nbytes for g in circ)
         d2h = x.nbytes + al.nbytes
-    e2e_total = sum(e2e_t)
-    if dist is not None:
-        tt = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
-        uu = torch.tensor([float(sum(e2e_u))], dtype=torch.float64, device=dev)
-        dist.all_reduce(uu, op=dist.ReduceOp.SUM)
-        e2e_value = float(uu.item()) / e2e_total
-    else:
-        e2e_value = sum(e2e_u) / e2e_total
+    e2e_total, e2e_units = over_ranks(dist, dev, sum(e2e_t), float(sum(e2e_u)))
+    e2e_value = e2e_units / e2e_total
 
     roofline = None
     kernels = None
@@ -324,6 +308,19 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
             "note": "algorithmic bytes = 24 B per entry read + 24 B per entry written; timing from a "
                     "profiled step (CUDA events around each launch on its stream)"}
     return roof, kernels[:12]
+
+
+def over_ranks(dist, dev, seconds, units):
+    """The job's time (max over ranks) and units (sum over ranks); replicas
+    share nothing else."""
+    if dist is None:
+        return float(seconds), float(units)
+    import torch
+    tt = torch.tensor([float(seconds)], dtype=torch.float64, device=dev)
+    uu = torch.tensor([float(units)], dtype=torch.float64, device=dev)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    dist.all_reduce(uu, op=dist.ReduceOp.SUM)
+    return float(tt.item()), float(uu.item())
 
 
 def main():
