@@ -35,7 +35,7 @@ CTRL_DTYPE = np.dtype([("gamma_running", "<f8"), ("state_gamma", "<f8"), ("pr_cu
                        ("last_truncated", "<i4"), ("amp_updates", "<i8"), ("n_trunc", "<i8"),
                        ("n_ops", "<i8"), ("accept", "<i4", (64,)), ("frac", "<f8", (64,)),
                        ("trace", "<u8"), ("trace_cap", "<i8"), ("trace_len", "<i8"),
-                       ("pr_tie_tol", "<f8"), ("sync_counter", "<u4"), ("pad1", "<i4"),
+                       ("pr_tie_tol", "<f8"), ("sync_counter", "<u4"), ("wait_limit", "<i4"),
                        ("prof_in", "<i8", (48,)), ("prof_out", "<i8", (48,))], align=True)
 PROF_SLOTS = 48
 KINDS = ["gate1", "rot1", "gate2", "perm", "plain", "rdm"]
@@ -108,6 +108,7 @@ def load_library():
         "bass_rdm_2q": (I32, [P, P, I32, I32, P, P, P, SZ, P]),
         "bass_to_dense": (I32, [P, P, I32, P, P, P]),
         "bass_dense_dot": (I32, [P, P, I64, P, P, P, SZ, P]),
+        "bass_dense_gate": (I32, [P, I32, P, I32, I32, I32, P]),
         "bass_sparse_dot": (I32, [P, P, I32, P, P, P, SZ, P]),
         "bass_rotate_step": (I32, [P, P, P, I32, I64, I32, P, P, SZ, P]),
         "bass_fingerprint": (I32, [P, D, P, P, SZ, P]),

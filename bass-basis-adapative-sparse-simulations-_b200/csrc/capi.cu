@@ -290,6 +290,13 @@ int bass_to_dense(const bass_state* st, const double* host_U, int nq, double* ps
   return status_of(run_to_dense(st, host_U, nq, psi, ctrl, (cudaStream_t)stream));
 }
 
+int bass_dense_gate(double* psi, int nq, const double* host_G, int gate_qubits, int q1, int q2, void* stream) {
+  if (!psi || !host_G || nq < 1 || nq > 34 || (gate_qubits != 1 && gate_qubits != 2) || q1 < 0 || q1 >= nq)
+    return BASS_ERR_ARG;
+  if (gate_qubits == 2 && (nq < 2 || q2 < 0 || q2 >= nq || q2 == q1)) return BASS_ERR_ARG;
+  return status_of(run_dense_gate(psi, nq, host_G, gate_qubits, q1, q2, (cudaStream_t)stream));
+}
+
 int bass_dense_dot(const double* u, const double* v, int64_t n, double* out, bass_ctrl* ctrl, void* ws,
                    size_t ws_bytes, void* stream) {
   if (!u || !v || !out || !ctrl || n < 0) return BASS_ERR_ARG;

@@ -43,6 +43,13 @@ __device__ __forceinline__ void set_error(bass_ctrl* c, int code) {
   atomicOr(&c->error, 1 << code);
 }
 
+// Spins a bounded wait makes before it gives up (bass_ctrl.wait_limit: 0 the
+// default kSpinLimit, > 0 that many, < 0 none).
+__device__ __forceinline__ long long wait_limit(const bass_ctrl* c) {
+  const int w = *(volatile const int*)&c->wait_limit;
+  return w == 0 ? kSpinLimit : (w < 0 ? 0 : (long long)w);
+}
+
 // ---------------------------------------------------------------------------
 // exact accumulation
 // ---------------------------------------------------------------------------
@@ -393,10 +400,11 @@ __device__ __forceinline__ long long lookback(unsigned long long* status, long l
   long long excl = 0;
   long long k = tile - 1;
   long long spins = 0;
+  const long long lim = wait_limit(ctrl);
   while (true) {
     unsigned long long s = ld_acquire(&status[k]);
     if ((s >> 62) == 0) {
-      if (++spins > kSpinLimit) {
+      if (++spins > lim) {
         set_error(ctrl, BASS_ERR_WAIT);
         break;
       }
@@ -427,12 +435,13 @@ __device__ __forceinline__ long long lookback_warp(unsigned long long* status, l
   long long base = tile - 1;
   long long spins = 0;
   bool gave_up = false;
+  const long long lim = wait_limit(ctrl);
   while (true) {
     const long long k = base - lane;
     unsigned long long s;
     do {
       s = (k >= 0 && !gave_up) ? ld_acquire(&status[k]) : kFlagInc;
-      if (++spins > kSpinLimit) gave_up = true;
+      if (++spins > lim) gave_up = true;
     } while (__any_sync(0xffffffffu, (s >> 62) == 0));
     const unsigned inc = __ballot_sync(0xffffffffu, (s >> 62) == 2);
     const int stop = inc ? __ffs(inc) - 1 : 32;

@@ -109,6 +109,10 @@ cudaError_t run_commit(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const 
                        cudaStream_t s);
 
 // misc.cu
+struct DenseG4 {
+  double2 m[16];
+};
+cudaError_t run_dense_gate(double* psi, int nq, const double* host_G, int nqg, int q1, int q2, cudaStream_t s);
 cudaError_t run_reduce(const bass_state* st, int mode, double* dest, bass_ctrl* ctrl,
                        const WsView& ws, cudaStream_t s);
 cudaError_t run_fingerprint(const bass_state* st, double pmin, uint64_t* out6, const WsView& ws,

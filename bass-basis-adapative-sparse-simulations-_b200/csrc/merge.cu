@@ -29,6 +29,8 @@
 // are emitted in child-index order, groups in Z order.
 #include <math.h>
 
+#include <atomic>
+
 #include "internal.h"
 
 namespace bass {
@@ -910,8 +912,9 @@ __device__ bool grid_sync(const OpArgs& a) {
       st_release(gen, g + 1);
     } else {
       long long spins = 0;
+      const long long lim = wait_limit(a.ctrl);
       while (ld_acquire(gen) == g) {
-        if (++spins > kSpinLimit) {
+        if (++spins > lim) {
           set_error(a.ctrl, BASS_ERR_WAIT);
           ok = 0;
           break;
@@ -1768,10 +1771,40 @@ cudaError_t zero_small(const WsView& ws, cudaStream_t s) {
   return cudaMemsetAsync(ws.counters, 0, bytes, s);
 }
 
+// A cooperative launch (the runtime guarantees that every block of the grid
+// is resident at once, or refuses the launch), as a programmatic dependent
+// launch where the runtime accepts both attributes together; otherwise a
+// plain cooperative launch.  The choice is made on the first launch and kept.
+template <typename... K, typename... A>
+static cudaError_t launch_coop(void (*kern)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                               A&&... args) {
+  static std::atomic<int> with_pdl{1};
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  if (with_pdl.load(std::memory_order_relaxed)) {
+    cfg.numAttrs = 2;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, args...);
+    if (e == cudaSuccess) return e;
+    cudaGetLastError();  // refused before launch: clear it and launch without PDL
+    with_pdl.store(0, std::memory_order_relaxed);
+  }
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
 // Launch of the selection; grid = every block that fits on the GPU at once
-// (its grid barriers need them all resident).  It is a programmatic
-// dependent launch: each block waits until the evaluation pass has completed,
-// and by then that pass has left every SM, so all blocks fit together.
+// (its grid barriers need them all resident), launched cooperatively so that
+// the runtime guarantees that residency.  Where it is also a programmatic
+// dependent launch, each block waits until the evaluation pass has completed.
 template <bool P2>
 static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace,
                                    cudaStream_t s) {
@@ -1791,7 +1824,7 @@ static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode,
   a.prof = prof_on() ? 1 : 0;
   dim3 grd(grid), blk(kSelThreads);
   cudaError_t e = cudaSuccess;
-  KLAUNCH(S_SELECT1, s, e = launch_pdl(k_select_coop<P2>, grd, blk, smem, s, a, ns, kind, gh, mode, j, trace));
+  KLAUNCH(S_SELECT1, s, e = launch_coop(k_select_coop<P2>, grd, blk, smem, s, a, ns, kind, gh, mode, j, trace));
   return e;
 }
 

@@ -591,6 +591,33 @@ __global__ void k_dense_1q(double2* psi, long long half, int j, double2 u00, dou
   }
 }
 
+// A 4x4 gate G (index (b_q1 << 1) | b_q2, row-major) applied to qubits
+// (q1, q2) of a dense vector of 4 quarter entries: each group of four
+// amplitudes is read, multiplied and written back by one thread, the sum over
+// input indices in ascending order (exact_simulator.py:121-144).
+__global__ void k_dense_2q(double2* psi, long long quarter, int q1, int q2, const __grid_constant__ DenseG4 g) {
+  const int lo = q1 < q2 ? q1 : q2, hi = q1 < q2 ? q2 : q1;
+  const long long mlo = (1LL << lo) - 1, mhi = (1LL << (hi - 1)) - 1;
+  const long long b1 = 1LL << q1, b2 = 1LL << q2;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < quarter;
+       p += (long long)gridDim.x * blockDim.x) {
+    // insert zero bits at positions lo and hi
+    long long i = ((p & ~mlo) << 1) | (p & mlo);
+    i = ((i & ~mhi) << 1) | (i & mhi);
+    const long long idx[4] = {i, i | b2, i | b1, i | b1 | b2};
+    double2 a[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) a[r] = psi[idx[r]];
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      double2 acc = cmul(g.m[o * 4], a[0]);
+#pragma unroll
+      for (int r = 1; r < 4; ++r) acc = cadd(acc, cmul(g.m[o * 4 + r], a[r]));
+      psi[idx[o]] = acc;
+    }
+  }
+}
+
 // Per-CTA exact partial sums of conj(u_i) v_i (re, im) into ws.red[2 b ..];
 // sparse: u is psi at the state's true keys and v its amplitudes.
 template <bool SPARSE>
@@ -673,6 +700,23 @@ cudaError_t run_to_dense(const bass_state* st, const double* host_U, int nq, dou
               k_dense_1q<<<grid, 256, 0, s>>>(p, n / 2, j, make_double2(u[0], u[1]), make_double2(u[2], u[3]),
                                                make_double2(u[4], u[5]), make_double2(u[6], u[7])));
     }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t run_dense_gate(double* psi, int nq, const double* host_G, int nqg, int q1, int q2, cudaStream_t s) {
+  double2* p = reinterpret_cast<double2*>(psi);
+  const int grid = device().sms * 8;
+  const double* u = host_G;
+  if (nqg == 1) {
+    KLAUNCH(S_SMALL, s,
+            k_dense_1q<<<grid, 256, 0, s>>>(p, (1LL << nq) / 2, q1, make_double2(u[0], u[1]),
+                                             make_double2(u[2], u[3]), make_double2(u[4], u[5]),
+                                             make_double2(u[6], u[7])));
+  } else {
+    DenseG4 g;
+    for (int i = 0; i < 16; ++i) g.m[i] = make_double2(u[2 * i], u[2 * i + 1]);
+    KLAUNCH(S_SMALL, s, k_dense_2q<<<grid, 256, 0, s>>>(p, (1LL << nq) / 4, q1, q2, g));
   }
   return cudaGetLastError();
 }

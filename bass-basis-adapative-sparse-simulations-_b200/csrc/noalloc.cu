@@ -11,6 +11,9 @@
 // Limits and rules:
 //   * the state may hold at most kNoAllocMaxEntries (2^20) entries; larger
 //     requests are refused with BASS_ERR_WORKSPACE before any work is queued;
+//     a state that does not fit the scratch although max_entries said it
+//     would is refused by the kernels themselves (BASS_ERR_WORKSPACE in ctrl,
+//     NaN in rho);
 //   * the array (about 4.8 MB) is part of the library image: every GPU that
 //     loads the library holds it until the process exits;
 //   * all calls share the one array: calls that may overlap on the GPU (other
@@ -19,7 +22,8 @@
 //     is fully rewritten by each call;
 //   * the first call on a device resolves the array's device address
 //     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture begins.
+//     before any stream capture begins.  The address is cached for the life
+//     of the process; it is not valid after cudaDeviceReset.
 #include <stddef.h>
 
 #include <mutex>

@@ -94,7 +94,10 @@ typedef struct bass_ctrl {
   int64_t trace_len;
   double pr_tie_tol;      /* a rotation must lower PR by more than this (rel.) */
   uint32_t sync_counter;  /* last-block bookkeeping of in-place kernels        */
-  int32_t pad1;
+  int32_t wait_limit;     /* spins of a bounded device wait before it gives up:
+                             0 the default (2^22), > 0 that many, < 0 none (a
+                             wait that is not already satisfied gives up at once;
+                             for tests of the give-up path)                      */
   int64_t prof_in[BASS_PROF_SLOTS];   /* entries read per kernel slot (profiling on) */
   int64_t prof_out[BASS_PROF_SLOTS];  /* entries written per kernel slot            */
 } bass_ctrl;
@@ -214,6 +217,12 @@ int bass_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* r
    qubits than nq sets BASS_ERR_ARG and is skipped. */
 int bass_to_dense(const bass_state* st, const double* host_U, int nq, double* psi, bass_ctrl* ctrl,
                   void* stream);
+/* exact_simulator.py:114-144 ExactSimulator._apply_1qubit_dense /
+   _apply_2qubit_dense: a gate applied in place to a dense statevector psi
+   (2^nq complex128, device, nq <= 34).  gate_qubits 1: host_G is 2x2 on qubit
+   q1 (q2 ignored); 2: host_G is 4x4, index (bit_q1 << 1) | bit_q2.  Each
+   output is a sum over input indices in ascending order, without FMA. */
+int bass_dense_gate(double* psi, int nq, const double* host_G, int gate_qubits, int q1, int q2, void* stream);
 /* runner.py:620-626 np.vdot(u, v) of two device complex128 vectors of n
    entries: out[0..1] = sum conj(u_i) v_i, exact sums (device doubles). */
 int bass_dense_dot(const double* u, const double* v, int64_t n, double* out, bass_ctrl* ctrl, void* ws,
@@ -228,10 +237,14 @@ int bass_sparse_dot(const bass_state* st, const double* psi, int nq, double* out
    the reference.  The scratch is a static array inside the library (about
    4.8 MB, held on every GPU that loads the library until exit); the state may
    hold at most 2^20 entries (max_entries is the caller's bound on st->nnz;
-   larger values return BASS_ERR_WORKSPACE).  All calls share the array, so
-   calls that may overlap on the GPU race and must be serialised.  The first
-   call on a device looks up the array's address; make it before any stream
-   capture.  Allocates nothing. */
+   larger values return BASS_ERR_WORKSPACE).  A state that does not fit the
+   scratch although max_entries said it would (more than 516 merge tiles,
+   about 1,052,640 entries) is refused on the device: the call returns
+   BASS_OK, ctrl->error gets BASS_ERR_WORKSPACE and rho gets NaN.  All calls
+   share the array, so calls that may overlap on the GPU race and must be
+   serialised.  The first call on a device looks up the array's address; make
+   it before any stream capture.  The address is kept for the life of the
+   process: it does not survive cudaDeviceReset.  Allocates nothing. */
 int bass_rdm_1q_noalloc(const bass_state* st, int64_t max_entries, int num_qubits, double* rho,
                         bass_ctrl* ctrl, void* stream);
 /* One coordinate-descent step of bass_simulator.py:755-814: rotate qubit j of

@@ -1,6 +1,12 @@
 """Generate the golden fixtures in this directory by running the reference.
 
-Usage:  python tests/golden/make_golden.py [--reference /path/to/reference]
+Usage:  python tests/golden/make_golden.py --reference /path/to/reference [mode]
+
+The reference checkout is given by ``--reference`` or the ``BASS_REFERENCE``
+environment variable.  Modes: (none) the kernel vectors and the BASS /
+FixedBasisSimulator runs; ``--only-2q`` the 2-qubit rotation fixtures;
+``--only-k14`` the brickwork run at n=40, depth 10, K=2^14;
+``--only-dense`` the reference's dense statevectors (ExactSimulator).
 
 The reference (Skill0issue/BASS-Basis-Adapative-Sparse-Simulations-, pure
 Python + Numba) is copied to a temporary directory (Numba's ``cache=True``
@@ -62,7 +68,9 @@ def import_reference(ref_dir):
     import src.simulation.bass_simulator as bs
     import src.simulation.simulator as fs
     import src.utils.random_circuits as rc
-    return dict(ss=ss, tr=tr, gates=gates, bs=bs, fs=fs, rc=rc)
+    import src.simulation.exact_simulator as ex
+    import src.benchmarking.fidelity as fid
+    return dict(ss=ss, tr=tr, gates=gates, bs=bs, fs=fs, rc=rc, ex=ex, fid=fid)
 
 
 class GapRecorder:
@@ -328,6 +336,62 @@ def main_2q(R, pkg):
               "min_gap", float(r["min_gap"]), f"{float(r['seconds']):.2f}s")
 
 
+def write_bass_cases(R, cases):
+    """Run each case on the tie-patched and on the unmodified reference and
+    store both traces (the unmodified one as raw_*)."""
+    for name, N, k, circ, kw in cases:
+        r = run_bass(R, N, k, circ, patched=True, **kw)
+        raw = run_bass(R, N, k, circ, patched=False, **kw)
+        meta, mats = gate_arrays(circ)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), N=np.int64(N), k=np.int64(k),
+                            kwargs=np.array(repr(kw)), gate_meta=meta, gate_mats=mats,
+                            pr_tie_tol=np.float64(PR_TIE_TOL), **r,
+                            **{f"raw_{key}": raw[key] for key in ("events", "gamma", "min_gap", "n_trunc")})
+        print(name, "events", len(r["events"]), "nnz", len(r["x"]), "gamma", float(r["gamma"]),
+              "raw gamma", float(raw["gamma"]), "min_gap", float(r["min_gap"]), "n_trunc",
+              int(r["n_trunc"]), f"{float(r['seconds']):.2f}s", flush=True)
+
+
+def main_dense(R, pkg):
+    """The reference's dense FP64 statevectors (ExactSimulator,
+    exact_simulator.py:66-144): two small circuits in full, and config 1
+    (TFIM n=24, 20 layers) at the keys of the config-1 BASS fixture, with the
+    reference's compute_fidelity (fidelity.py:48-65) of that fixture's state."""
+    ex = R["ex"].ExactSimulator
+    out = {}
+    small = [("brick_n12", 12, pkg.circuits.brickwork_circuit(12, 10, rng=np.random.default_rng(4))),
+             ("tfim_n14", 14, pkg.circuits.tfim_circuit(14, 6, J=1.0, h=1.0, dt=0.3, rng=np.random.default_rng(9),
+                                                        disorder_strength_h=0.5))]
+    np.random.seed(17)
+    small.append(("haar2q_n10", 10, R["rc"].generate_random_circuit(10, 8)))
+    for name, N, circ in small:
+        meta, mats = gate_arrays(circ)
+        out[f"{name}_N"] = np.int64(N)
+        out[f"{name}_gate_meta"] = meta
+        out[f"{name}_gate_mats"] = mats
+        out[f"{name}_psi"] = ex(N, verbose=False).simulate(circ)
+        print(name, "done", flush=True)
+    z = np.load(os.path.join(HERE, "config1_tfim_n24_k65536.npz"))
+    circ = pkg.circuits.config1_circuit(seed=0)
+    t0 = time.perf_counter()
+    psi = ex(24, verbose=False).simulate(circ)
+    dt = time.perf_counter() - t0
+    x = z["x"]
+    st = R["ss"].SparseState(24, len(x))
+    st.x = x.copy(); st.alpha = z["a"].copy(); st.nnz = len(x); st.gamma = float(z["gamma"])
+    out["config1_x"] = x
+    out["config1_psi_at_x"] = psi[x.astype(np.int64)]
+    out["config1_fidelity"] = np.float64(R["fid"].compute_fidelity(st, psi))
+    top = np.argsort(-np.abs(psi))[:256]
+    out["config1_top_idx"] = top.astype(np.int64)
+    out["config1_top_psi"] = psi[top]
+    out["config1_norm2"] = np.float64(np.vdot(psi, psi).real)
+    out["config1_seconds"] = np.float64(dt)
+    np.savez_compressed(os.path.join(HERE, "dense_exact.npz"), **out)
+    print("dense_exact.npz: config-1 fidelity", float(out["config1_fidelity"]), "gamma^2",
+          float(z["gamma"]) ** 2, f"{dt:.1f}s", flush=True)
+
+
 def oracle_free_haar(rng):
     z = (rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))) / np.sqrt(2.0)
     q, r = np.linalg.qr(z)
@@ -337,15 +401,27 @@ def oracle_free_haar(rng):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("BASS_REFERENCE"),
+                    help="the reference checkout (default: $BASS_REFERENCE)")
     ap.add_argument("--skip-large", action="store_true")
     ap.add_argument("--only-2q", action="store_true", help="write only the 2-qubit rotation fixtures")
+    ap.add_argument("--only-k14", action="store_true", help="write only the n=40 depth-10 K=2^14 run")
+    ap.add_argument("--only-dense", action="store_true", help="write only the dense statevector fixtures")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give the reference checkout with --reference or $BASS_REFERENCE")
     oracle.build()
     R = import_reference(args.reference)
     pkg = load_pkg()
     if args.only_2q:
         main_2q(R, pkg)
+        return
+    if args.only_k14:
+        write_bass_cases(R, [("config2_brick_n40_d10_k16384", 40, 2 ** 14,
+                              pkg.circuits.config2_circuit(seed=0, depth=10), {})])
+        return
+    if args.only_dense:
+        main_dense(R, pkg)
         return
     rng = np.random.default_rng(20261203)
 
@@ -380,17 +456,7 @@ def main():
         cases.append(("config1_tfim_n24_k65536", 24, 2 ** 16, c_pkg, {}))
         cases.append(("config2_brick_n40_d30_k1024", 40, 2 ** 10, pkg.circuits.config2_circuit(seed=0), {}))
         cases.append(("config2_brick_n40_d12_k4096", 40, 2 ** 12, pkg.circuits.config2_circuit(seed=1, depth=12), {}))
-    for name, N, k, circ, kw in cases:
-        r = run_bass(R, N, k, circ, patched=True, **kw)
-        raw = run_bass(R, N, k, circ, patched=False, **kw)
-        meta, mats = gate_arrays(circ)
-        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), N=np.int64(N), k=np.int64(k),
-                            kwargs=np.array(repr(kw)), gate_meta=meta, gate_mats=mats,
-                            pr_tie_tol=np.float64(PR_TIE_TOL), **r,
-                            **{f"raw_{key}": raw[key] for key in ("events", "gamma", "min_gap", "n_trunc")})
-        print(name, "events", len(r["events"]), "nnz", len(r["x"]), "gamma", float(r["gamma"]),
-              "raw gamma", float(raw["gamma"]), "min_gap", float(r["min_gap"]), "n_trunc",
-              int(r["n_trunc"]), f"{float(r['seconds']):.2f}s")
+    write_bass_cases(R, cases)
 
     # FixedBasisSimulator: top-k and random-k (seeded)
     for name, trunc in [("fixed_topk_n12_k64", "top-k"), ("fixed_randk_n12_k64", "random-k")]:

@@ -9,7 +9,8 @@ key-set fingerprint must be identical.
 import numpy as np
 import pytest
 
-from _common import BASS_CASES, LARGE_CASES, first_mismatch, load_case, sig_events, sorted_state
+from _common import (BASS_CASES, FULL_MATCH_CASES, LARGE_CASES, agreeing_prefix, first_mismatch, full_events,
+                     load_case, sig_events, sorted_state)
 
 pytestmark = pytest.mark.gpu
 
@@ -311,6 +312,34 @@ def test_bass_matches_reference_goldens(B, name):
     fid = abs(np.vdot(z["a"], st.alpha)) ** 2
     assert fid >= 1 - 1e-10
     assert abs(st.gamma - float(z["gamma"])) <= 1e-9 * float(z["gamma"])
+
+
+@pytest.mark.parametrize("name", FULL_MATCH_CASES)
+def test_bass_full_key_sets_match_reference(B, name):
+    """Every event in full (the fingerprint of all keys, the nnz, accept and
+    optimisation events) equals the tie-patched reference's."""
+    z, circ, kw = load_case(name)
+    b, st = _gpu_bass(B, z, circ, kw)
+    assert first_mismatch(full_events(b.trace_events()), full_events(z["events"])) is None
+
+
+@pytest.mark.parametrize("name", BASS_CASES + LARGE_CASES)
+def test_bass_matches_unpatched_reference(B, name):
+    """Against the unmodified reference (np.argpartition, `pr_new >= pr`):
+    identical significant key sets at every event up to the first event at
+    which the unmodified and the tie-patched reference themselves part (a
+    rotation whose PR change is rounding noise, or a tie at the top-k
+    boundary); for config 1 and the other runs where they never part, the
+    whole trace."""
+    z, circ, kw = load_case(name)
+    b, _ = _gpu_bass(B, z, circ, kw)
+    mine = sig_events(b.trace_events())
+    raw, patched = sig_events(z["raw_events"]), sig_events(z["events"])
+    n = agreeing_prefix(raw, patched)
+    assert n > 0
+    assert mine[:n] == raw[:n]
+    if raw == patched:
+        assert mine == raw
 
 
 @pytest.mark.parametrize("name", ["fixed_topk_n12_k64"])

@@ -40,3 +40,18 @@ def test_host_formulas(pkg):
     assert metrics.estimate_cross_entropy_fidelity(st, exact, 300) == ref_x
     # runner.py:620-626 (the vdot part)
     assert metrics.dense_overlap(exact, exact) == complex(np.vdot(exact, exact))
+
+
+def test_fidelity_bass_above_24_qubits_is_zero(pkg):
+    # runner.py:620-626 returns 0.0 for N > 24 without building a statevector
+    from bass_b200 import metrics
+
+    class FakeSim:
+        def __init__(self, N):
+            self.N = N
+
+        def to_statevector_device(self, state):
+            raise AssertionError("no statevector above 24 qubits")
+
+    for N in (25, 30, 40):
+        assert metrics.fidelity_bass(FakeSim(N), None, None) == 0.0

@@ -11,7 +11,8 @@ against the tie-patched reference (see make_golden.py).
 import numpy as np
 import pytest
 
-from _common import BASS_CASES, LARGE_CASES, first_mismatch, load_case, sig_events, sorted_state
+from _common import (BASS_CASES, BASS2Q_CASES, FULL_MATCH_CASES, LARGE_CASES, first_mismatch, full_events,
+                     load_case, sig_events, sorted_state)
 
 RTOL = 1e-13   # relative amplitude tolerance for per-kernel comparisons
 
@@ -171,3 +172,13 @@ def test_fixed_basis(orc, name):
     close(as_, z["a"], 1e-10)
     assert np.array_equal(f.nnz_history, z["nnz_hist"])
     assert np.allclose(f.gamma_history ** 2, z["gamma_sq_hist"], rtol=1e-10, atol=0)
+
+
+@pytest.mark.parametrize("name", FULL_MATCH_CASES)
+def test_bass_full_key_sets_match_reference(orc, name):
+    """Every event, including the fingerprint of all keys (not only the
+    significant ones), equals the reference's."""
+    z, circ, kw = load_case(name)
+    tr = orc.Trace()
+    orc.OracleBASS(int(z["N"]), int(z["k"]), trace=tr, **kw).simulate(circ)
+    assert first_mismatch(full_events(tr.array()), full_events(z["events"])) is None

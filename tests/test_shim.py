@@ -8,7 +8,7 @@ import pytest
 
 from conftest import ROOT
 
-REF = os.environ.get("BASS_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("BASS_REFERENCE", "")
 
 
 def _make_golden():
@@ -19,7 +19,7 @@ def _make_golden():
     return m
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="the reference sources are not on this machine")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="set BASS_REFERENCE to a reference checkout")
 @pytest.mark.filterwarnings("ignore::SyntaxWarning")   # a docstring escape in the reference's runner
 def test_reference_runner_uses_gpu_classes(pkg):
     mg = _make_golden()

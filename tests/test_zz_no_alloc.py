@@ -91,3 +91,31 @@ def test_noalloc_refuses_large_states(lib):
     rc = lib.bass_rdm_1q_noalloc(st._cur.ptr, MAX_ENTRIES + 1, 20, ctypes.c_void_p(_native._ptr(out)),
                                  eng.ctrl_ptr, eng.stream)
     assert rc == _native.ERR_WORKSPACE
+
+
+def test_noalloc_refuses_oversized_state_on_device(lib):
+    # max_entries understates the state: the host check passes and the
+    # kernels' own tile-count guards refuse the state (no scratch is touched
+    # beyond its bounds): error bit in ctrl, NaN moments, status still OK
+    import torch
+    from bass_b200 import _native
+    from bass_b200.state import SparseState
+    N, n = 40, 1_100_000
+    rng = np.random.default_rng(5)
+    x = np.unique(rng.integers(0, 2 ** N, size=n + 1000, dtype=np.uint64))[:n]
+    a = rng.standard_normal(len(x)) + 1j * rng.standard_normal(len(x))
+    st = SparseState(N, len(x), _capacity=len(x) + 16)
+    st.load(x, a)
+    assert st.nnz == n
+    eng = st._eng
+    out = torch.zeros(4 * N, dtype=torch.float64, device=eng.device)
+    rc = lib.bass_rdm_1q_noalloc(st._cur.ptr, MAX_ENTRIES, N, ctypes.c_void_p(_native._ptr(out)),
+                                 eng.ctrl_ptr, eng.stream)
+    assert rc == 0
+    with pytest.raises(_native.BassError, match="workspace"):
+        eng.raise_on_error()
+    assert np.isnan(out.cpu().numpy()).all()
+    # the library is still usable afterwards: a state that fits gives the
+    # workspace entry point's moments
+    st2 = make_state(6, 24, 30000)
+    assert np.array_equal(rdm_noalloc(lib, st2, 24), rdm_with_workspace(st2, 24))
