@@ -18,6 +18,17 @@ _lib = None
 
 TRACE_WORDS = 7
 SIG_PMIN = 1e-24
+AMP_C128, AMP_C64 = 0, 1   # bass_state.amp_type
+
+
+def amp_type_of(dtype) -> int:
+    """BASS_AMP_* of a numpy complex dtype (complex128 or complex64)."""
+    dt = np.dtype(dtype)
+    if dt == np.complex128:
+        return AMP_C128
+    if dt == np.complex64:
+        return AMP_C64
+    raise ValueError(f"amplitudes must be complex128 or complex64, not {dt}")
 
 # status codes / error bits
 OK, ERR_CAPACITY, ERR_WAIT, ERR_ARG, ERR_CUDA, ERR_WORKSPACE = 0, 1, 2, 3, 4, 5
@@ -27,7 +38,7 @@ _ERR_NAMES = {ERR_CAPACITY: "capacity overflow", ERR_WAIT: "bounded device wait 
 
 # numpy mirrors of the device descriptors (C layout, natural alignment)
 STATE_DTYPE = np.dtype([("keys", "<u8"), ("amps", "<u8"), ("nnz", "<i8"), ("cap", "<i8"),
-                        ("rscale", "<f8", (2,)), ("nq", "<i4"), ("pad0", "<i4"),
+                        ("rscale", "<f8", (2,)), ("nq", "<i4"), ("amp_type", "<i4"),
                         ("pos", "i1", (64,)), ("qat", "i1", (64,))], align=True)
 CTRL_DTYPE = np.dtype([("gamma_running", "<f8"), ("state_gamma", "<f8"), ("pr_cur", "<f8"),
                        ("pr_last", "<f8"), ("last_kept", "<f8"), ("last_total", "<f8"),
@@ -87,6 +98,9 @@ def load_library():
         "bass_ctrl_bytes": (SZ, []),
         "bass_workspace_bytes": (SZ, [I64, I64, I32]),
         "bass_state_init": (I32, [P, P, P, I64, I32, ctypes.c_uint64, P]),
+        "bass_state_init_typed": (I32, [P, P, P, I64, I32, ctypes.c_uint64, I32, P]),
+        "bass_state_import_typed": (I32, [P, P, P, I64, P, P, I64, I32, I32, P, SZ, P, P]),
+        "bass_state_export_typed": (I32, [P, P, P, I32, I32, P, SZ, P, P]),
         "bass_state_import_into": (I32, [P, P, P, I64, P, P, I64, I32, P, SZ, P, P]),
         "bass_state_export": (I32, [P, P, P, P, SZ, P, P]),
         "bass_state_export_bits": (I32, [P, P, P, I32, P, SZ, P, P]),
@@ -243,25 +257,33 @@ class Engine:
 
 
 class DevState:
-    """One device descriptor plus its key / amplitude buffers."""
+    """One device descriptor plus its key / amplitude buffers (complex128, or
+    complex64 with ``amp_type=AMP_C64``)."""
 
-    def __init__(self, eng: Engine, cap: int, init_key: int = 0):
+    def __init__(self, eng: Engine, cap: int, init_key: int = 0, amp_type: int = AMP_C128):
         torch = eng.torch
         self.eng = eng
         self.cap = int(max(cap, 1))
+        self.amp_type = int(amp_type)
         self.desc = torch.zeros(eng.L.bass_state_bytes(), dtype=torch.uint8, device=eng.device)
         self.keys = torch.zeros(self.cap, dtype=torch.int64, device=eng.device)
-        self.amps = torch.zeros(2 * self.cap, dtype=torch.float64, device=eng.device)
+        ft = torch.float32 if self.amp_type == AMP_C64 else torch.float64
+        self.amps = torch.zeros(2 * self.cap, dtype=ft, device=eng.device)
         self.init(init_key)
+
+    @property
+    def np_dtype(self):
+        return np.complex64 if self.amp_type == AMP_C64 else np.complex128
 
     @property
     def ptr(self):
         return ctypes.c_void_p(_ptr(self.desc))
 
     def init(self, key: int = 0):
-        check(self.eng.L.bass_state_init(self.ptr, ctypes.c_void_p(_ptr(self.keys)),
-                                         ctypes.c_void_p(_ptr(self.amps)), self.cap, self.eng.nq,
-                                         ctypes.c_uint64(int(key)), self.eng.stream), "bass_state_init")
+        check(self.eng.L.bass_state_init_typed(self.ptr, ctypes.c_void_p(_ptr(self.keys)),
+                                               ctypes.c_void_p(_ptr(self.amps)), self.cap, self.eng.nq,
+                                               ctypes.c_uint64(int(key)), self.amp_type, self.eng.stream),
+              "bass_state_init")
 
     def read_desc(self):
         return np.frombuffer(self.desc.cpu().numpy().tobytes(), dtype=STATE_DTYPE)[0]
@@ -276,13 +298,13 @@ class DevState:
         n = int(self.read_desc()["nnz"])
         torch = eng.torch
         ok = torch.empty(max(n, 1), dtype=torch.int64, device=eng.device)
-        oa = torch.empty(2 * max(n, 1), dtype=torch.float64, device=eng.device)
+        oa = torch.empty(2 * max(n, 1), dtype=self.amps.dtype, device=eng.device)
         bits = eng.nq if key_bits is None else key_bits
-        check(eng.L.bass_state_export_bits(self.ptr, ctypes.c_void_p(_ptr(ok)), ctypes.c_void_p(_ptr(oa)),
-                                           int(bits), eng.ws_ptr, eng.ws_bytes, eng.ctrl_ptr, eng.stream),
-              "bass_state_export")
+        check(eng.L.bass_state_export_typed(self.ptr, ctypes.c_void_p(_ptr(ok)), ctypes.c_void_p(_ptr(oa)),
+                                            int(bits), self.amp_type, eng.ws_ptr, eng.ws_bytes, eng.ctrl_ptr,
+                                            eng.stream), "bass_state_export")
         x = ok[:n].cpu().numpy().view(np.uint64).copy()
-        a = oa[:2 * n].cpu().numpy().view(np.complex128).copy()
+        a = oa[:2 * n].cpu().numpy().view(self.np_dtype).copy()
         return x, a
 
     def load(self, x, a):
@@ -290,16 +312,17 @@ class DevState:
         eng = self.eng
         torch = eng.torch
         x = np.ascontiguousarray(x, dtype=np.uint64)
-        a = np.ascontiguousarray(a, dtype=np.complex128)
+        a = np.ascontiguousarray(a, dtype=self.np_dtype)
         n = len(x)
         if n > self.cap:
             raise BassError("state capacity exceeded")
+        real = np.float32 if self.amp_type == AMP_C64 else np.float64
         kx = torch.from_numpy(x.view(np.int64).copy()).to(eng.device) if n else self.keys
-        ka = torch.from_numpy(a.view(np.float64).copy()).to(eng.device) if n else self.amps
-        check(eng.L.bass_state_import_into(self.ptr, ctypes.c_void_p(_ptr(self.keys)),
-                                           ctypes.c_void_p(_ptr(self.amps)), self.cap,
-                                           ctypes.c_void_p(_ptr(kx)), ctypes.c_void_p(_ptr(ka)), n, eng.nq,
-                                           eng.ws_ptr, eng.ws_bytes, eng.ctrl_ptr, eng.stream),
+        ka = torch.from_numpy(a.view(real).copy()).to(eng.device) if n else self.amps
+        check(eng.L.bass_state_import_typed(self.ptr, ctypes.c_void_p(_ptr(self.keys)),
+                                            ctypes.c_void_p(_ptr(self.amps)), self.cap,
+                                            ctypes.c_void_p(_ptr(kx)), ctypes.c_void_p(_ptr(ka)), n, eng.nq,
+                                            self.amp_type, eng.ws_ptr, eng.ws_bytes, eng.ctrl_ptr, eng.stream),
               "bass_state_import_into")
         eng.torch.cuda.current_stream(eng.device).synchronize()  # kx / ka are temporaries
 

@@ -12,6 +12,15 @@ depends on nnz).  With the default ``truncate_every=1`` the simulate-level
 truncation (keep the top k, gamma_running *= kept/total, renormalise) is
 fused into the gate's kernels and decided on the device.
 
+Precision form: ``dtype=np.complex64`` stores the amplitudes as complex64
+(16-byte entries instead of 24).  Gate and rotation arithmetic is then FP32
+with compensated products and sums (each output rounded once), while |a|^2,
+the norm, the top-k threshold, the discarded weight, the PR and the RDM
+moments behind the rotation-angle solve stay FP64 (exact sums on the device,
+the 2x2 eigen-solve and the frames on the host).  ``record_truncations=True``
+keeps, per simulate-level truncation, (gate index, kept mass, total mass) in
+``self.truncations`` (one synchronising read per gate, for reports).
+
 One deliberate difference: a basis rotation is kept only if it lowers the
 participation ratio by more than ``pr_tie_tol`` (relative, default 1e-12).
 The reference keeps it on any decrease, so rotations that leave PR unchanged
@@ -31,7 +40,7 @@ class BASS:
     def __init__(self, num_qubits, k, optimize_every=5, buffer_factor=2, truncate_every=1, max_nnz_factor=8,
                  use_2qubit_rotations=False, verbose=False, use_fast_eigh=True, use_diag_gate=True,
                  use_kron_cache=True, pr_opt_threshold=0.90, *, pr_tie_tol=1e-12, trace=False,
-                 trace_cap=None):
+                 trace_cap=None, dtype=np.complex128, record_truncations=False):
         self.N = num_qubits
         self.k = k
         self.optimize_every = optimize_every
@@ -47,6 +56,10 @@ class BASS:
         self.pr_tie_tol = pr_tie_tol
         self.trace = bool(trace)
         self.trace_cap = trace_cap
+        self.dtype = np.dtype(dtype)
+        nat.amp_type_of(self.dtype)
+        self.record_truncations = bool(record_truncations)
+        self.truncations = []
         self._kron_cache = {}
         self.U = None
         self._gamma_running = 1.0
@@ -169,14 +182,18 @@ class BASS:
         fast = self.truncate_every == 1
         cap = (min(k, 2 ** N) + 16) if fast else 4 * hard_cap + 16
         tcap = self.trace_cap if self.trace_cap is not None else (4 * len(circuit) * (N + 4) + 1024 if self.trace else 0)
-        state = SparseState(N, internal_k, initial_state, _capacity=cap, _trace_cap=tcap)
+        state = SparseState(N, internal_k, initial_state, dtype=self.dtype, _capacity=cap, _trace_cap=tcap)
         eng = state._eng
         M = len(circuit)
         gates_since = 0
         tr_flag = int(self.trace)
         fused = nat.trunc(k, k, 1, 1, 1, tr_flag)
         internal = nat.trunc(internal_k, internal_k, 3, 2, 0, 0)
+        self.truncations = []
+        n_trunc_seen = 0
         for i, gate in enumerate(circuit):
+            if self.record_truncations and i > 0:
+                n_trunc_seen = self._record(eng, i - 1, n_trunc_seen)
             self.stats["gates"] += 1
             if gate.n_qubits == 1:
                 q = gate.qubits[0]
@@ -204,6 +221,8 @@ class BASS:
             else:
                 raise ValueError(f"{gate.n_qubits}-qubit gates unsupported")
             self._maybe_optimize(state, i, M)
+        if self.record_truncations and M:
+            self._record(eng, M - 1, n_trunc_seen)
         c = eng.read_ctrl()
         eng.raise_on_error()
         self._gamma_running = float(c["gamma_running"])
@@ -212,6 +231,14 @@ class BASS:
         self.stats["truncations"] = int(c["n_trunc"])
         self.last_state = state
         return state
+
+    def _record(self, eng, i, seen):
+        """Append gate i's simulate-level truncation, if it made one."""
+        c = eng.read_ctrl()
+        n = int(c["n_trunc"])
+        if n > seen and int(c["last_truncated"]):
+            self.truncations.append((i, float(c["last_kept"]), float(c["last_total"])))
+        return n
 
     def _maybe_optimize(self, state, i, M):
         if self.optimize_every > 0 and (i + 1) % self.optimize_every == 0 and i + 1 < M:

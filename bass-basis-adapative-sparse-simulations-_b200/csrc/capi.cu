@@ -168,38 +168,56 @@ size_t bass_workspace_bytes(int64_t max_in, int64_t max_out, int num_qubits) {
   return ws_bytes_for(m);
 }
 
-int bass_state_init(bass_state* st, uint64_t* keys, double* amps, int64_t cap, int num_qubits,
-                    uint64_t init_key, void* stream) {
-  if (!st || !keys || !amps || cap < 1 || num_qubits < 1 || num_qubits > BASS_MAX_QUBITS)
+static bool amp_type_ok(int t) { return t == BASS_AMP_C128 || t == BASS_AMP_C64; }
+
+int bass_state_init_typed(bass_state* st, uint64_t* keys, double* amps, int64_t cap, int num_qubits,
+                          uint64_t init_key, int amp_type, void* stream) {
+  if (!st || !keys || !amps || cap < 1 || num_qubits < 1 || num_qubits > BASS_MAX_QUBITS || !amp_type_ok(amp_type))
     return BASS_ERR_ARG;
   if (num_qubits < 64 && (init_key >> num_qubits) != 0) return BASS_ERR_ARG;
-  return status_of(run_state_init(st, keys, amps, cap, num_qubits, init_key, (cudaStream_t)stream));
+  return status_of(run_state_init(st, keys, amps, cap, num_qubits, init_key, amp_type, (cudaStream_t)stream));
+}
+
+int bass_state_init(bass_state* st, uint64_t* keys, double* amps, int64_t cap, int num_qubits,
+                    uint64_t init_key, void* stream) {
+  return bass_state_init_typed(st, keys, amps, cap, num_qubits, init_key, BASS_AMP_C128, stream);
+}
+
+int bass_state_import_typed(bass_state* st, uint64_t* st_keys, double* st_amps, int64_t cap,
+                            const uint64_t* keys, const double* amps, int64_t n, int num_qubits, int amp_type,
+                            void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
+  if (!st || !st_keys || !st_amps || (n > 0 && (!keys || !amps)) || n < 0 || n > cap || num_qubits < 1 ||
+      num_qubits > BASS_MAX_QUBITS || !ctrl || !amp_type_ok(amp_type))
+    return BASS_ERR_ARG;
+  CHECK_WS(ws, ws_bytes, v);
+  if (n > v.max_n) return BASS_ERR_WORKSPACE;
+  return status_of(run_import(st, keys, amps, n, num_qubits, v, ctrl, (cudaStream_t)stream, st_keys,
+                              st_amps, cap, amp_type));
 }
 
 int bass_state_import_into(bass_state* st, uint64_t* st_keys, double* st_amps, int64_t cap,
                            const uint64_t* keys, const double* amps, int64_t n, int num_qubits,
                            void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
-  if (!st || !st_keys || !st_amps || (n > 0 && (!keys || !amps)) || n < 0 || n > cap || num_qubits < 1 ||
-      num_qubits > BASS_MAX_QUBITS || !ctrl)
+  return bass_state_import_typed(st, st_keys, st_amps, cap, keys, amps, n, num_qubits, BASS_AMP_C128, ws,
+                                 ws_bytes, ctrl, stream);
+}
+
+int bass_state_export_typed(const bass_state* st, uint64_t* out_keys, double* out_amps, int key_bits,
+                            int amp_type, void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
+  if (!st || !out_keys || !out_amps || !ctrl || key_bits < 1 || key_bits > 64 || !amp_type_ok(amp_type))
     return BASS_ERR_ARG;
   CHECK_WS(ws, ws_bytes, v);
-  if (n > v.max_n) return BASS_ERR_WORKSPACE;
-  return status_of(run_import(st, keys, amps, n, num_qubits, v, ctrl, (cudaStream_t)stream, st_keys,
-                              st_amps, cap));
+  return status_of(run_export(st, out_keys, out_amps, key_bits, v, ctrl, (cudaStream_t)stream, amp_type));
 }
 
 int bass_state_export(const bass_state* st, uint64_t* out_keys, double* out_amps, void* ws,
                       size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
-  if (!st || !out_keys || !out_amps || !ctrl) return BASS_ERR_ARG;
-  CHECK_WS(ws, ws_bytes, v);
-  return status_of(run_export(st, out_keys, out_amps, 64, v, ctrl, (cudaStream_t)stream));
+  return bass_state_export_typed(st, out_keys, out_amps, 64, BASS_AMP_C128, ws, ws_bytes, ctrl, stream);
 }
 
 int bass_state_export_bits(const bass_state* st, uint64_t* out_keys, double* out_amps, int key_bits,
                            void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
-  if (!st || !out_keys || !out_amps || !ctrl || key_bits < 1 || key_bits > 64) return BASS_ERR_ARG;
-  CHECK_WS(ws, ws_bytes, v);
-  return status_of(run_export(st, out_keys, out_amps, key_bits, v, ctrl, (cudaStream_t)stream));
+  return bass_state_export_typed(st, out_keys, out_amps, key_bits, BASS_AMP_C128, ws, ws_bytes, ctrl, stream);
 }
 
 int bass_state_copy_desc(bass_state* dst, const bass_state* src, void* stream) {
@@ -421,8 +439,7 @@ int bass_radix_sort_u64(uint64_t* keys, double* amps, int64_t n, int key_bits, v
   if ((n > 0 && (!keys || !amps)) || n < 0 || key_bits < 1 || key_bits > 64) return BASS_ERR_ARG;
   CHECK_WS(ws, ws_bytes, v);
   if (n > v.max_n) return BASS_ERR_WORKSPACE;
-  return status_of(run_radix_sort(keys, reinterpret_cast<double2*>(amps), n, nullptr, key_bits, v, ctrl,
-                                  (cudaStream_t)stream));
+  return status_of(run_radix_sort(keys, amps, n, nullptr, key_bits, v, ctrl, (cudaStream_t)stream, 0));
 }
 
 int bass_merge_sorted(uint64_t* keys, double* amps, int64_t n, int64_t* n_out, void* ws, size_t ws_bytes,

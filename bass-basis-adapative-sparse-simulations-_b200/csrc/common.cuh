@@ -220,6 +220,66 @@ __device__ __forceinline__ double2 scale_load(double2 a, double r0, double r1) {
 }
 
 // ---------------------------------------------------------------------------
+// amplitude storage (bass_state.amp_type)
+// ---------------------------------------------------------------------------
+// A complex64 entry is read as the double2 of its float parts (exact).  Its
+// value with a pending renormalisation is the scaled value rounded back to
+// complex64, so every reader sees what the materialised state would hold.
+__device__ __forceinline__ double2 f2d(float2 v) { return make_double2((double)v.x, (double)v.y); }
+__device__ __forceinline__ float2 d2f(double2 v) {
+  return make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
+}
+__device__ __forceinline__ double2 amp_raw(const double* amps, long long i, int c64) {
+  return c64 ? f2d(reinterpret_cast<const float2*>(amps)[i]) : reinterpret_cast<const double2*>(amps)[i];
+}
+__device__ __forceinline__ double2 amp_scale(double2 raw, int c64, double r0, double r1) {
+  const double2 v = scale_load(raw, r0, r1);
+  return c64 ? f2d(d2f(v)) : v;
+}
+__device__ __forceinline__ double2 amp_get(const double* amps, long long i, int c64, double r0, double r1) {
+  return amp_scale(amp_raw(amps, i, c64), c64, r0, r1);
+}
+// stores v (a complex64 state rounds it to float parts)
+__device__ __forceinline__ void amp_put(double* amps, long long i, double2 v, int c64) {
+  if (c64) reinterpret_cast<float2*>(amps)[i] = d2f(v);
+  else reinterpret_cast<double2*>(amps)[i] = v;
+}
+
+// FP32 gate arithmetic of complex64 states: the compensated dot product Dot2
+// of Ogita, Rump and Oishi ("Accurate sum and dot product", SIAM J. Sci.
+// Comput. 26(6), 2005), built from Knuth's TwoSum and the fused-multiply-add
+// TwoProduct.  Every product's rounding error and every addition's rounding
+// error are carried in a second float and added back once, so a sum of
+// complex products is as accurate as if evaluated in twice the precision and
+// then rounded to float.
+struct Dot2f {
+  float s, c;
+};
+__device__ __forceinline__ void dot2_add(Dot2f& d, float x, float y) {
+  const float p = __fmul_rn(x, y);
+  const float pe = __fmaf_rn(x, y, -p);  // x*y - p, exactly
+  const float t = __fadd_rn(d.s, p);
+  const float z = __fsub_rn(t, d.s);
+  const float se = __fadd_rn(__fsub_rn(d.s, __fsub_rn(t, z)), __fsub_rn(p, z));  // s + p - t, exactly
+  d.s = t;
+  d.c = __fadd_rn(d.c, __fadd_rn(pe, se));
+}
+__device__ __forceinline__ float dot2_get(const Dot2f& d) { return __fadd_rn(d.s, d.c); }
+// (re, im) += g * a
+__device__ __forceinline__ void cdot2_add(Dot2f& re, Dot2f& im, float2 g, float2 a) {
+  dot2_add(re, g.x, a.x);
+  dot2_add(re, -g.y, a.y);
+  dot2_add(im, g.x, a.y);
+  dot2_add(im, g.y, a.x);
+}
+// g * a of float-valued complex numbers, rounded once to complex64 (as double2)
+__device__ __forceinline__ double2 cmul_c64(double2 g, double2 a) {
+  Dot2f re{0.f, 0.f}, im{0.f, 0.f};
+  cdot2_add(re, im, d2f(g), d2f(a));
+  return make_double2((double)dot2_get(re), (double)dot2_get(im));
+}
+
+// ---------------------------------------------------------------------------
 // keys
 // ---------------------------------------------------------------------------
 __host__ __device__ __forceinline__ uint64_t fmix64(uint64_t z) {

@@ -117,19 +117,19 @@ cudaError_t run_reduce(const bass_state* st, int mode, double* dest, bass_ctrl* 
                        const WsView& ws, cudaStream_t s);
 cudaError_t run_fingerprint(const bass_state* st, double pmin, uint64_t* out6, const WsView& ws,
                             cudaStream_t s, bass_ctrl* ctrl, int append_event, int only_if_trunc);
-cudaError_t run_radix_sort(uint64_t* keys, double2* amps, long long n, const long long* n_dev,
-                           int key_bits, const WsView& ws, bass_ctrl* ctrl, cudaStream_t s);
+cudaError_t run_radix_sort(uint64_t* keys, double* amps, long long n, const long long* n_dev,
+                           int key_bits, const WsView& ws, bass_ctrl* ctrl, cudaStream_t s, int c64);
 cudaError_t run_renorm(bass_state* st, bass_ctrl* ctrl, const WsView& ws, cudaStream_t s);
 cudaError_t run_phase2q(bass_state* st, const double* d, int q1, int q2, bass_ctrl* ctrl, cudaStream_t s);
 cudaError_t run_phase1q(bass_state* st, bass_state* tmp, const double* g, int q, bass_ctrl* ctrl,
                         const WsView& ws, cudaStream_t s);
 cudaError_t run_state_init(bass_state* st, uint64_t* keys, double* amps, long long cap, int nq,
-                           uint64_t key, cudaStream_t s);
+                           uint64_t key, int amp_type, cudaStream_t s);
 cudaError_t run_import(bass_state* st, const uint64_t* keys, const double* amps, long long n, int nq,
                        const WsView& ws, bass_ctrl* ctrl, cudaStream_t s, uint64_t* st_keys,
-                       double* st_amps, long long cap);
+                       double* st_amps, long long cap, int amp_type);
 cudaError_t run_export(const bass_state* st, uint64_t* ok, double* oa, int key_bits, const WsView& ws,
-                       bass_ctrl* ctrl, cudaStream_t s);
+                       bass_ctrl* ctrl, cudaStream_t s, int amp_type);
 cudaError_t run_merge_sorted(uint64_t* keys, double* amps, long long n, long long* n_out,
                              const WsView& ws, bass_ctrl* ctrl, cudaStream_t s);
 cudaError_t run_clone(bass_state* dst, const bass_state* src, bass_ctrl* ctrl, cudaStream_t s);

@@ -43,6 +43,7 @@ struct Hdr {
   double r0, r1;
   int t;
   int nq;
+  int c64;  // the state stores complex64 amplitudes
   int8_t qat_out[64];
 };
 
@@ -211,13 +212,16 @@ __device__ __forceinline__ bool above_drop(double2 c) {
 // read at Z position p through the merge's permutation (identity when there
 // is none), with the state's pending renormalisation applied.
 struct AmpView {
-  const double2* sA;
+  const double2* sA;   // complex128 amplitudes in load order, or
+  const float2* sAf;   // complex64 amplitudes (c64)
   const uint16_t* sP;  // Z position -> load position, or nullptr
   double r0, r1;
   bool scaled;
+  bool c64;
   __device__ __forceinline__ double2 operator()(int p) const {
-    const double2 v = sA[sP ? (int)sP[p] : p];
-    return scaled ? scale_load(v, r0, r1) : v;
+    const int q = sP ? (int)sP[p] : p;
+    const double2 v = c64 ? f2d(sAf[q]) : sA[q];
+    return scaled ? amp_scale(v, c64 ? 1 : 0, r0, r1) : v;
   }
 };
 
@@ -225,7 +229,7 @@ struct AmpView {
 // start one).  G is the op's gate matrix, read from the kernel's parameter
 // block (k_tile takes its arguments as a __grid_constant__), so every lane
 // loads the same constant-bank words.
-template <int KIND>
+template <int KIND, bool F32>
 __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t* sZ, const AmpView& sA, int gb,
                                                    const double2* G, int drop_zero, uint64_t* base,
                                                    double2* ca) {
@@ -252,6 +256,42 @@ __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t*
     ar[r] = in ? sA(p + r) : make_double2(0.0, 0.0);
   }
   unsigned mask = 0;
+  if (F32) {
+    // complex64: float gate entries and amplitudes, compensated FP32 sums
+    // (Dot2); a contribution counts when neither factor is zero
+    if (KIND == K_GATE1 || KIND == K_GATE2) {
+#pragma unroll
+      for (int o = 0; o < NC; ++o) {
+        Dot2f re{0.f, 0.f}, im{0.f, 0.f};
+        bool have = false;
+#pragma unroll
+        for (int r = 0; r < NC; ++r) {
+          if (lr[r] < 0) continue;
+          const float2 g = d2f(G[o * NC + lr[r]]), x = d2f(ar[r]);
+          if (!((g.x != 0.f || g.y != 0.f) && (x.x != 0.f || x.y != 0.f))) continue;
+          cdot2_add(re, im, g, x);
+          have = true;
+        }
+        const double2 acc = make_double2((double)dot2_get(re), (double)dot2_get(im));
+        ca[o] = acc;
+        if (drop_zero == 2 ? above_drop(acc) : have) mask |= 1u << o;
+      }
+    } else if (KIND == K_ROT1) {
+      const float2 zero = make_float2(0.f, 0.f);
+      const float2 a0 = (lr[0] == 0) ? d2f(ar[0]) : zero;
+      const float2 a1 = (lr[0] == 1) ? d2f(ar[0]) : (lr[1] == 1 ? d2f(ar[1]) : zero);
+#pragma unroll
+      for (int o = 0; o < 2; ++o) {
+        Dot2f re{0.f, 0.f}, im{0.f, 0.f};
+        cdot2_add(re, im, d2f(G[o * 2]), a0);
+        cdot2_add(re, im, d2f(G[o * 2 + 1]), a1);
+        const double2 c = make_double2((double)dot2_get(re), (double)dot2_get(im));
+        ca[o] = c;
+        if (above_drop(c)) mask |= 1u << o;
+      }
+    }
+    return mask;
+  }
   if (KIND == K_GATE1 || KIND == K_GATE2) {
 #pragma unroll
     for (int o = 0; o < NC; ++o) {
@@ -282,6 +322,15 @@ __device__ __forceinline__ unsigned group_children(int p, int E, const uint64_t*
     }
   }
   return mask;
+}
+
+// group_children for the state's amplitude type
+template <int KIND>
+__device__ __forceinline__ unsigned group_children_t(bool c64, int p, int E, const uint64_t* sZ, const AmpView& sA,
+                                                     int gb, const double2* G, int drop_zero, uint64_t* base,
+                                                     double2* ca) {
+  return c64 ? group_children<KIND, true>(p, E, sZ, sA, gb, G, drop_zero, base, ca)
+             : group_children<KIND, false>(p, E, sZ, sA, gb, G, drop_zero, base, ca);
 }
 
 __device__ __forceinline__ bool keep_child(uint64_t bits, uint64_t key, const SelState& S,
@@ -328,6 +377,7 @@ __device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int
     nw = 0;
   }
   out->nq = in->nq;
+  out->amp_type = in->amp_type;
   out->nnz = nw;
   out->rscale[0] = 1.0;
   out->rscale[1] = 1.0;
@@ -463,6 +513,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
     H.r0 = in->rscale[0];
     H.r1 = in->rscale[1];
     H.nq = in->nq;
+    H.c64 = in->amp_type == BASS_AMP_C64;
     H.t = (KIND == K_IDENT || KIND == K_RDM) ? 0 : in->pos[a.q];
     H.ntiles = (KIND == K_IDENT) ? plain_tiles(H.n) : merge_tiles(H.n);
   }
@@ -542,6 +593,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
       const int o1 = (int)sSegOff[1], o2 = (int)sSegOff[2], o3 = (int)sSegOff[3], o4 = (int)sSegOff[4];
       const unsigned zb = (unsigned)__cvta_generic_to_shared(sZ);
       const unsigned ab = (unsigned)__cvta_generic_to_shared(sA);
+      const bool c64 = H.c64;
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
         const int e = k * kThreads + tid;
@@ -549,8 +601,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
           const int sg = (e >= o1) + (e >= o2) + (e >= o3) + (e >= o4);
           const long long src = sSegLo[sg] + (e - sSegOff[sg]);
           asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(zb + 8u * e), "l"(H.keys + src) : "memory");
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(ab + 16u * e), "l"(H.amps + src)
-                       : "memory");
+          if (c64)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(ab + 8u * e),
+                         "l"(reinterpret_cast<const float2*>(H.amps) + src)
+                         : "memory");
+          else
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(ab + 16u * e), "l"(H.amps + src)
+                         : "memory");
         }
       }
       asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
@@ -642,7 +699,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
       __syncthreads();
     }
 
-    const AmpView amp{sA, KIND == K_IDENT ? nullptr : sPerm, H.r0, H.r1, scaled};
+    const bool c64 = H.c64 != 0;
+    const AmpView amp{sA, reinterpret_cast<const float2*>(sA), KIND == K_IDENT ? nullptr : sPerm, H.r0, H.r1,
+                      scaled, c64};
 
     // ---- evaluate ------------------------------------------------------------
     // Round r gives position r * kThreads + tid to thread tid, so neighbouring
@@ -741,7 +800,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
         if (wmode == 2) {
           mk = 1u;
         } else {
-          const unsigned cm = group_children<KIND>(p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
+          const unsigned cm = group_children_t<KIND>(c64, p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
           if ((cm & 1u) && keep_child((uint64_t)__double_as_longlong(prob(ca[0])), kb, S, H.qat_out)) mk = 1u;
         }
         sMask[p] = (uint8_t)mk;
@@ -784,17 +843,17 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
       // (d) write the kept children
       if (sBase + tile_total <= a.out->cap) {
         uint64_t* ok = a.out->keys;
-        double2* oa = reinterpret_cast<double2*>(a.out->amps);
+        double* oa = a.out->amps;
         for (int p = tid; p < E; p += kThreads) {
           const unsigned mk = sMask[p];
           if (!mk) continue;
           long long o = sBase + sOff[p];
-          group_children<KIND>(p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
+          group_children_t<KIND>(c64, p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
 #pragma unroll
           for (int c = 0; c < MC; ++c) {
             if ((mk >> c) & 1u) {
               ok[o] = kb | (uint64_t)c;
-              oa[o] = ca[c];
+              amp_put(oa, o, ca[c], c64);
               ++o;
             }
           }
@@ -809,8 +868,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
       unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys) + NS * sZstart;
       uint64_t* skeys = a.ws.stage_keys + NS * sZstart;
       double2* samps = a.ws.tmp_amps + NS * sZstart;
+      float2* sampf = reinterpret_cast<float2*>(a.ws.tmp_amps) + NS * sZstart;
       for (int p = tid; p < E; p += kThreads) {
-        const unsigned cm = group_children<KIND>(p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
+        const unsigned cm = group_children_t<KIND>(c64, p, E, sZ, amp, gb, a.G, a.drop_zero, &kb, ca);
         unsigned long long sb[NS];
 #pragma unroll
         for (int c = 0; c < NS; ++c) {
@@ -824,14 +884,23 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
         if (cm) {  // every slot of the group is written (a missing child's slot holds ~0 bits)
           if (NS == 1) {
             skeys[p] = kb;
-            samps[p] = ca[0];
+            if (c64) sampf[p] = d2f(ca[0]);
+            else samps[p] = ca[0];
           } else {
 #pragma unroll
             for (int c = 0; c < NS; c += 2)
               *reinterpret_cast<ulonglong2*>(skeys + (long long)NS * p + c) =
                   make_ulonglong2(kb | (uint64_t)c, kb | (uint64_t)(c + 1));
+            if (c64) {
 #pragma unroll
-            for (int c = 0; c < NS; ++c) samps[(long long)NS * p + c] = ca[c];
+              for (int c = 0; c < NS; c += 2) {
+                const float2 f0 = d2f(ca[c]), f1 = d2f(ca[c + 1]);
+                *reinterpret_cast<float4*>(sampf + (long long)NS * p + c) = make_float4(f0.x, f0.y, f1.x, f1.y);
+              }
+            } else {
+#pragma unroll
+              for (int c = 0; c < NS; ++c) samps[(long long)NS * p + c] = ca[c];
+            }
           }
         }
         if (NS == 1) {
@@ -1609,6 +1678,9 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs 
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
   uint64_t* okeys = a.out->keys;
   double2* oamps = reinterpret_cast<double2*>(a.out->amps);
+  float2* oampf = reinterpret_cast<float2*>(a.out->amps);
+  const float2* stf = reinterpret_cast<const float2*>(a.ws.tmp_amps);
+  const bool c64 = a.in->amp_type == BASS_AMP_C64;
   const long long cap = a.out->cap;
   const unsigned lt = (1u << lane) - 1;
   long long written = 0;
@@ -1654,7 +1726,12 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs 
         bal[u] = __ballot_sync(0xffffffffu, kept);
         if (kept) {
           kk[u] = __ldcs(a.ws.stage_keys + i);
-          aa[u] = __ldcs(a.ws.tmp_amps + i);
+          if (c64) {
+            const float2 f = __ldcs(stf + i);
+            aa[u] = make_double2(f.x, f.y);
+          } else {
+            aa[u] = __ldcs(a.ws.tmp_amps + i);
+          }
         }
         if (lane == 0) sCnt[u][w] = __popc(bal[u]);
       }
@@ -1679,7 +1756,8 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs 
           if ((bal[u] >> lane) & 1u) {
             const long long o = base + ahead + __popc(bal[u] & lt);
             okeys[o] = kk[u];
-            oamps[o] = aa[u];
+            if (c64) oampf[o] = make_float2((float)aa[u].x, (float)aa[u].y);  // float values: exact
+            else oamps[o] = aa[u];
           }
         }
       } else if (tid == 0) {

@@ -17,7 +17,7 @@ __global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsVi
   __shared__ i128 sRed[8];
   const long long n = st->nnz;
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  const double2* amps = reinterpret_cast<const double2*>(st->amps);
+  const int c64 = st->amp_type == BASS_AMP_C64;
   i128 v[1] = {0};
   // eight entries per thread and round, summed exactly in the split
   // accumulators (fx_acc96) and joined once per round
@@ -27,12 +27,12 @@ __global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsVi
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const long long i = i0 + u * stride;
-      x[u] = i < n ? amps[i] : make_double2(0.0, 0.0);
+      x[u] = i < n ? amp_raw(st->amps, i, c64) : make_double2(0.0, 0.0);
     }
     double h = 0.0, l = 0.0;
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const double p = prob(scale_load(x[u], r0, r1));
+      const double p = prob(amp_scale(x[u], c64, r0, r1));
       fx_acc96(MODE == R_NORM2 ? p : __dmul_rn(p, p), h, l, v[0]);
     }
     v[0] += fx_join96s(h, l);
@@ -89,10 +89,10 @@ __global__ void k_materialize(bass_state* st, WsView ws, bass_ctrl* c) {
   if (ws.sel->pad != 3) return;
   const long long n = st->nnz;
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  double2* amps = reinterpret_cast<double2*>(st->amps);
+  const int c64 = st->amp_type == BASS_AMP_C64;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
-    amps[i] = scale_load(amps[i], r0, r1);
+    amp_put(st->amps, i, amp_get(st->amps, i, c64, r0, r1), c64);
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -114,14 +114,14 @@ __global__ void __launch_bounds__(256) k_fingerprint(const bass_state* st, doubl
   __syncthreads();
   const long long n = st->nnz;
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  const double2* amps = reinterpret_cast<const double2*>(st->amps);
+  const int c64 = st->amp_type == BASS_AMP_C64;
   unsigned long long c = 0, s = 0, x = 0, c2 = 0, s2 = 0, x2 = 0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const uint64_t tk = true_key(st->keys[i], qat, 64);
     const uint64_t f1 = fmix64(tk), f2 = fmix64(tk ^ kFpSalt);
     ++c; s += f1; x ^= f2;
-    if (prob(scale_load(amps[i], r0, r1)) > pmin) { ++c2; s2 += f1; x2 ^= f2; }
+    if (prob(amp_get(st->amps, i, c64, r0, r1)) > pmin) { ++c2; s2 += f1; x2 ^= f2; }
   }
   for (int off = 16; off > 0; off >>= 1) {
     c += __shfl_down_sync(0xffffffffu, c, off);
@@ -160,14 +160,15 @@ __global__ void k_phase2q(bass_state* st, double2 d0, double2 d1, double2 d2, do
   const long long n = st->nnz;
   const int t1 = st->pos[q1], t2 = st->pos[q2];
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  double2* amps = reinterpret_cast<double2*>(st->amps);
+  const int c64 = st->amp_type == BASS_AMP_C64;
   const uint64_t* keys = st->keys;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const uint64_t y = keys[i];
     const int idx = (int)((((y >> t1) & 1ULL) << 1) | ((y >> t2) & 1ULL));
     const double2 d = idx == 0 ? d0 : idx == 1 ? d1 : idx == 2 ? d2 : d3;
-    amps[i] = cmul(scale_load(amps[i], r0, r1), d);
+    const double2 v = amp_get(st->amps, i, c64, r0, r1);
+    amp_put(st->amps, i, c64 ? cmul_c64(v, d) : cmul(v, d), c64);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -191,14 +192,15 @@ __global__ void k_phase1q(bass_state* st, double2 g0, double2 g1, int q, bass_ct
   const long long n = st->nnz;
   const int t = st->pos[q];
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  double2* amps = reinterpret_cast<double2*>(st->amps);
+  const int c64 = st->amp_type == BASS_AMP_C64;
   const uint64_t* keys = st->keys;
   bool zero = false;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const double2 g = ((keys[i] >> t) & 1ULL) ? g1 : g0;
-    const double2 v = cmul(g, scale_load(amps[i], r0, r1));
-    amps[i] = v;
+    const double2 a = amp_get(st->amps, i, c64, r0, r1);
+    const double2 v = c64 ? cmul_c64(g, a) : cmul(g, a);
+    amp_put(st->amps, i, v, c64);
     zero |= !cnz(v);
   }
   if (__any_sync(0xffffffffu, zero) && (threadIdx.x & 31) == 0) ws.sel->pad = 1;
@@ -234,7 +236,7 @@ __global__ void k_phase1q_fin(bass_state* st, bass_state* tmp, WsView ws) {
 // state set-up, copies, gathers
 // ---------------------------------------------------------------------------
 __global__ void k_state_init(bass_state* st, uint64_t* keys, double* amps, long long cap, int nq,
-                             uint64_t init_key) {
+                             uint64_t init_key, int amp_type) {
   st->keys = keys;
   st->amps = amps;
   st->nnz = 1;
@@ -242,15 +244,14 @@ __global__ void k_state_init(bass_state* st, uint64_t* keys, double* amps, long 
   st->rscale[0] = 1.0;
   st->rscale[1] = 1.0;
   st->nq = nq;
-  st->pad0 = 0;
+  st->amp_type = amp_type;
   for (int p = 0; p < 64; ++p) { st->pos[p] = (int8_t)p; st->qat[p] = (int8_t)p; }
   keys[0] = init_key;
-  amps[0] = 1.0;
-  amps[1] = 0.0;
+  amp_put(amps, 0, make_double2(1.0, 0.0), amp_type == BASS_AMP_C64);
 }
 
 __global__ void k_state_adopt(bass_state* st, uint64_t* keys, double* amps, long long cap, int nq,
-                              long long n) {
+                              long long n, int amp_type) {
   st->keys = keys;
   st->amps = amps;
   st->nnz = n;
@@ -258,6 +259,7 @@ __global__ void k_state_adopt(bass_state* st, uint64_t* keys, double* amps, long
   st->rscale[0] = 1.0;
   st->rscale[1] = 1.0;
   st->nq = nq;
+  st->amp_type = amp_type;
   for (int p = 0; p < 64; ++p) { st->pos[p] = (int8_t)p; st->qat[p] = (int8_t)p; }
 }
 
@@ -266,20 +268,19 @@ __global__ void k_copy_desc(bass_state* dst, const bass_state* src) { *dst = *sr
 // deep copy of entries; dst keeps its own buffers
 __global__ void k_clone(bass_state* dst, const bass_state* src, bass_ctrl* c) {
   const long long n = src->nnz;
-  if (n > dst->cap) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) set_error(c, BASS_ERR_CAPACITY);
+  if (n > dst->cap || dst->amp_type != src->amp_type) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_error(c, n > dst->cap ? BASS_ERR_CAPACITY : BASS_ERR_ARG);
     return;
   }
-  const double2* sa = reinterpret_cast<const double2*>(src->amps);
-  double2* da = reinterpret_cast<double2*>(dst->amps);
+  const int c64 = src->amp_type == BASS_AMP_C64;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     dst->keys[i] = src->keys[i];
-    da[i] = sa[i];
+    amp_put(dst->amps, i, amp_raw(src->amps, i, c64), c64);
   }
 }
 __global__ void k_clone_desc(bass_state* dst, const bass_state* src) {
-  if (src->nnz > dst->cap) return;
+  if (src->nnz > dst->cap || dst->amp_type != src->amp_type) return;
   dst->nnz = src->nnz;
   dst->rscale[0] = src->rscale[0];
   dst->rscale[1] = src->rscale[1];
@@ -294,18 +295,21 @@ __global__ void k_gather(const bass_state* in, bass_state* out, const int64_t* i
     return;
   }
   const long long nin = in->nnz;
-  const double2* ia = reinterpret_cast<const double2*>(in->amps);
-  double2* oa = reinterpret_cast<double2*>(out->amps);
+  const int c64 = in->amp_type == BASS_AMP_C64;
+  if (out->amp_type != in->amp_type) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_error(c, BASS_ERR_ARG);
+    return;
+  }
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const long long k = idx[i];
     if (k < 0 || k >= nin) { set_error(c, BASS_ERR_ARG); continue; }
     out->keys[i] = in->keys[k];
-    oa[i] = ia[k];
+    amp_put(out->amps, i, amp_raw(in->amps, k, c64), c64);
   }
 }
 __global__ void k_gather_desc(const bass_state* in, bass_state* out, long long n) {
-  if (n > out->cap) return;
+  if (n > out->cap || out->amp_type != in->amp_type) return;
   out->nnz = n;
   out->rscale[0] = in->rscale[0];
   out->rscale[1] = in->rscale[1];
@@ -314,18 +318,24 @@ __global__ void k_gather_desc(const bass_state* in, bass_state* out, long long n
 }
 
 // export: true keys and scaled amplitudes (sorted afterwards)
-__global__ void k_export(const bass_state* st, uint64_t* ok, double2* oa, long long max_n) {
+// (output amplitudes of the state's type; amp_type is what the caller expects)
+__global__ void k_export(const bass_state* st, uint64_t* ok, double* oa, long long max_n, int amp_type,
+                         bass_ctrl* c) {
   __shared__ int8_t qat[64];
   if (threadIdx.x < 64) qat[threadIdx.x] = st->qat[threadIdx.x];
   __syncthreads();
   const long long n = st->nnz;
   if (n > max_n) return;
+  if (st->amp_type != amp_type) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_error(c, BASS_ERR_ARG);
+    return;
+  }
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  const double2* amps = reinterpret_cast<const double2*>(st->amps);
+  const int c64 = amp_type == BASS_AMP_C64;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     ok[i] = true_key(st->keys[i], qat, 64);
-    oa[i] = scale_load(amps[i], r0, r1);
+    amp_put(oa, i, amp_get(st->amps, i, c64, r0, r1), c64);
   }
 }
 
@@ -389,8 +399,10 @@ __global__ void __launch_bounds__(1024) k_rs_scan(const long long* n_dev, long l
   }
 }
 
-__global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t* ik, const double2* ia, uint64_t* ok,
-                                                    double2* oa, const long long* n_dev, long long n_host,
+// P: the amplitude payload moved with each key (16 B complex128, 8 B complex64)
+template <typename P>
+__global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t* ik, const P* ia, uint64_t* ok,
+                                                    P* oa, const long long* n_dev, long long n_host,
                                                     int shift, WsView ws) {
   __shared__ unsigned int cntw[8][257];
   __shared__ unsigned int run[256];
@@ -409,7 +421,7 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t* ik, const do
       const long long i = lo + r * 256 + threadIdx.x;
       const bool valid = i < n;
       uint64_t key = 0;
-      double2 amp = make_double2(0.0, 0.0);
+      P amp{};
       unsigned dig = 256;
       if (valid) {
         key = ik[i];
@@ -437,7 +449,8 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t* ik, const do
   }
 }
 
-__global__ void k_copy_entries(const uint64_t* ik, const double2* ia, uint64_t* ok, double2* oa,
+template <typename P>
+__global__ void k_copy_entries(const uint64_t* ik, const P* ia, uint64_t* ok, P* oa,
                                const long long* n_dev, long long n_host) {
   const long long n = n_dev ? *n_dev : n_host;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -447,34 +460,44 @@ __global__ void k_copy_entries(const uint64_t* ik, const double2* ia, uint64_t* 
   }
 }
 
-cudaError_t run_radix_sort(uint64_t* keys, double2* amps, long long n_host, const long long* n_dev,
-                           int key_bits, const WsView& ws, bass_ctrl* ctrl, cudaStream_t s) {
-  (void)ctrl;
+template <typename P>
+static cudaError_t radix_sort_t(uint64_t* keys, P* amps, long long n_host, const long long* n_dev, int key_bits,
+                                const WsView& ws, cudaStream_t s) {
   const int grid = device().grid_small;
   uint64_t* ks = keys;
-  double2* as = amps;
+  P* as = amps;
   uint64_t* kd = ws.tmp_keys;
-  double2* ad = ws.tmp_amps;
+  P* ad = reinterpret_cast<P*>(ws.tmp_amps);
   int passes = 0;
   for (int shift = 0; shift < key_bits; shift += 8) {
     KLAUNCH(S_SORT, s, k_rs_hist<<<grid, 256, 0, s>>>(ks, n_dev, n_host, shift, ws));
     KLAUNCH(S_SORT, s, k_rs_scan<<<1, 1024, 0, s>>>(n_dev, n_host, ws));
-    KLAUNCH(S_SORT, s, k_rs_scatter<<<grid, 256, 0, s>>>(ks, as, kd, ad, n_dev, n_host, shift, ws));
+    KLAUNCH(S_SORT, s, k_rs_scatter<P><<<grid, 256, 0, s>>>(ks, as, kd, ad, n_dev, n_host, shift, ws));
     uint64_t* tk = ks; ks = kd; kd = tk;
-    double2* ta = as; as = ad; ad = ta;
+    P* ta = as; as = ad; ad = ta;
     ++passes;
   }
-  if (passes & 1) KLAUNCH(S_SORT, s, k_copy_entries<<<grid, 256, 0, s>>>(ks, as, keys, amps, n_dev, n_host));
+  if (passes & 1) KLAUNCH(S_SORT, s, k_copy_entries<P><<<grid, 256, 0, s>>>(ks, as, keys, amps, n_dev, n_host));
   return cudaGetLastError();
+}
+
+// amps: complex128 pairs, or complex64 pairs when c64
+cudaError_t run_radix_sort(uint64_t* keys, double* amps, long long n_host, const long long* n_dev, int key_bits,
+                           const WsView& ws, bass_ctrl* ctrl, cudaStream_t s, int c64) {
+  (void)ctrl;
+  if (c64)
+    return radix_sort_t(keys, reinterpret_cast<unsigned long long*>(amps), n_host, n_dev, key_bits, ws, s);
+  return radix_sort_t(keys, reinterpret_cast<ulonglong2*>(amps), n_host, n_dev, key_bits, ws, s);
 }
 
 // ---------------------------------------------------------------------------
 // sparse_state.py:127-147 merge_sorted_kernel: sum runs of equal keys (left to
 // right), one output per run, order kept (decoupled look-back on run heads)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_merge_runs(const uint64_t* keys, const double2* amps,
+// complex64 runs are summed in FP32 with the compensated (TwoSum) sum
+__global__ void __launch_bounds__(256) k_merge_runs(const uint64_t* keys, const double* amps,
                                                     const long long* n_dev, long long n_host, WsView ws,
-                                                    bass_ctrl* c) {
+                                                    bass_ctrl* c, int c64) {
   __shared__ long long sItem, sBase;
   __shared__ int sWarp[32];
   const long long n = n_dev ? *n_dev : n_host;
@@ -525,10 +548,20 @@ __global__ void __launch_bounds__(256) k_merge_runs(const uint64_t* keys, const 
     for (int k = 0; k < kPerThread; ++k) {
       const long long i = lo + k;
       if (i < n && (i == 0 || keys[i] != keys[i - 1])) {
-        double2 acc = amps[i];
-        for (long long r = i + 1; r < n && keys[r] == keys[i]; ++r) acc = cadd(acc, amps[r]);
+        double2 acc = amp_raw(amps, i, c64);
+        if (c64) {
+          Dot2f re{(float)acc.x, 0.f}, im{(float)acc.y, 0.f};
+          for (long long r = i + 1; r < n && keys[r] == keys[i]; ++r) {
+            const double2 v = amp_raw(amps, r, 1);
+            dot2_add(re, (float)v.x, 1.f);
+            dot2_add(im, (float)v.y, 1.f);
+          }
+          acc = make_double2((double)dot2_get(re), (double)dot2_get(im));
+        } else {
+          for (long long r = i + 1; r < n && keys[r] == keys[i]; ++r) acc = cadd(acc, amp_raw(amps, r, 0));
+        }
         ws.tmp_keys[o] = keys[i];
-        ws.tmp_amps[o] = acc;
+        amp_put(reinterpret_cast<double*>(ws.tmp_amps), o, acc, c64);
         ++o;
       }
     }
@@ -536,12 +569,12 @@ __global__ void __launch_bounds__(256) k_merge_runs(const uint64_t* keys, const 
   }
 }
 
-__global__ void k_merge_out(uint64_t* keys, double2* amps, WsView ws, long long* n_out, bass_state* st) {
+__global__ void k_merge_out(uint64_t* keys, double* amps, WsView ws, long long* n_out, bass_state* st, int c64) {
   const long long n = ws.sel->n_written;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     keys[i] = ws.tmp_keys[i];
-    amps[i] = ws.tmp_amps[i];
+    amp_put(amps, i, amp_raw(reinterpret_cast<const double*>(ws.tmp_amps), i, c64), c64);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (n_out) *n_out = n;
@@ -564,7 +597,7 @@ __global__ void k_dense_scatter(const bass_state* st, double2* psi, int nq, bass
   __syncthreads();
   const long long n = st->nnz;
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  const double2* amps = reinterpret_cast<const double2*>(st->amps);
+  const int c64 = st->amp_type == BASS_AMP_C64;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
   {
@@ -573,7 +606,7 @@ __global__ void k_dense_scatter(const bass_state* st, double2* psi, int nq, bass
       set_error(c, BASS_ERR_ARG);
       continue;
     }
-    psi[tk] = scale_load(amps[i], r0, r1);
+    psi[tk] = amp_get(st->amps, i, c64, r0, r1);
   }
 }
 
@@ -597,11 +630,12 @@ __global__ void k_dense_1q(double2* psi, long long half, int j, double2 u00, dou
 // input indices in ascending order (exact_simulator.py:121-144).
 __global__ void k_dense_2q(double2* psi, long long quarter, int q1, int q2, const __grid_constant__ DenseG4 g) {
   const int lo = q1 < q2 ? q1 : q2, hi = q1 < q2 ? q2 : q1;
-  const long long mlo = (1LL << lo) - 1, mhi = (1LL << (hi - 1)) - 1;
+  // p has nq - 2 bits: a zero is inserted at bit lo, then (in the nq - 1 bit
+  // result) at bit hi
+  const long long mlo = (1LL << lo) - 1, mhi = (1LL << hi) - 1;
   const long long b1 = 1LL << q1, b2 = 1LL << q2;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < quarter;
        p += (long long)gridDim.x * blockDim.x) {
-    // insert zero bits at positions lo and hi
     long long i = ((p & ~mlo) << 1) | (p & mlo);
     i = ((i & ~mhi) << 1) | (i & mhi);
     const long long idx[4] = {i, i | b2, i | b1, i | b1 | b2};
@@ -627,14 +661,14 @@ __global__ void __launch_bounds__(256) k_dot(const double2* u, const double2* v,
   __shared__ int8_t qat[64];
   long long nn = n;
   double r0 = 1.0, r1 = 1.0;
-  const double2* amps = v;
+  int c64 = 0;
   if (SPARSE) {
     if (threadIdx.x < 64) qat[threadIdx.x] = st->qat[threadIdx.x];
     __syncthreads();
     nn = st->nnz;
     r0 = st->rscale[0];
     r1 = st->rscale[1];
-    amps = reinterpret_cast<const double2*>(st->amps);
+    c64 = st->amp_type == BASS_AMP_C64;
   }
   i128 acc[2] = {0, 0};
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -652,7 +686,7 @@ __global__ void __launch_bounds__(256) k_dot(const double2* u, const double2* v,
           continue;
         }
         a = u[tk];
-        b = scale_load(amps[i], r0, r1);
+        b = amp_get(st->amps, i, c64, r0, r1);
       } else {
         a = u[i];
         b = v[i];
@@ -787,41 +821,41 @@ cudaError_t run_phase1q(bass_state* st, bass_state* tmp, const double* g, int q,
 }
 
 cudaError_t run_state_init(bass_state* st, uint64_t* keys, double* amps, long long cap, int nq,
-                           uint64_t key, cudaStream_t s) {
-  KLAUNCH(S_SMALL, s, k_state_init<<<1, 1, 0, s>>>(st, keys, amps, cap, nq, key));
+                           uint64_t key, int amp_type, cudaStream_t s) {
+  KLAUNCH(S_SMALL, s, k_state_init<<<1, 1, 0, s>>>(st, keys, amps, cap, nq, key, amp_type));
   return cudaGetLastError();
 }
 
 cudaError_t run_import(bass_state* st, const uint64_t* keys, const double* amps, long long n, int nq,
                        const WsView& ws, bass_ctrl* ctrl, cudaStream_t s, uint64_t* st_keys,
-                       double* st_amps, long long cap) {
+                       double* st_amps, long long cap, int amp_type) {
+  const int c64 = amp_type == BASS_AMP_C64;
   cudaError_t e = cudaMemcpyAsync(st_keys, keys, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
   if (e != cudaSuccess) return e;
-  e = cudaMemcpyAsync(st_amps, amps, n * 2 * sizeof(double), cudaMemcpyDeviceToDevice, s);
+  e = cudaMemcpyAsync(st_amps, amps, n * (c64 ? 2 * sizeof(float) : 2 * sizeof(double)), cudaMemcpyDeviceToDevice, s);
   if (e != cudaSuccess) return e;
-  KLAUNCH(S_SMALL, s, k_state_adopt<<<1, 1, 0, s>>>(st, st_keys, st_amps, cap, nq, n));
-  e = run_radix_sort(st_keys, reinterpret_cast<double2*>(st_amps), n, nullptr, nq > 0 ? nq : 1, ws, ctrl, s);
+  KLAUNCH(S_SMALL, s, k_state_adopt<<<1, 1, 0, s>>>(st, st_keys, st_amps, cap, nq, n, amp_type));
+  e = run_radix_sort(st_keys, st_amps, n, nullptr, nq > 0 ? nq : 1, ws, ctrl, s, c64);
   if (e != cudaSuccess) return e;
   if ((e = zero_small(ws, s)) != cudaSuccess) return e;
-  KLAUNCH(S_MERGE_RUNS, s, k_merge_runs<<<device().grid_small, 256, 0, s>>>(st_keys, reinterpret_cast<double2*>(st_amps), nullptr, n,
-                                                   ws, ctrl));
-  KLAUNCH(S_MERGE_RUNS, s, k_merge_out<<<device().grid_small, 256, 0, s>>>(st_keys, reinterpret_cast<double2*>(st_amps), ws, nullptr, st));
+  KLAUNCH(S_MERGE_RUNS, s, k_merge_runs<<<device().grid_small, 256, 0, s>>>(st_keys, st_amps, nullptr, n, ws, ctrl, c64));
+  KLAUNCH(S_MERGE_RUNS, s, k_merge_out<<<device().grid_small, 256, 0, s>>>(st_keys, st_amps, ws, nullptr, st, c64));
   return cudaGetLastError();
 }
 
 cudaError_t run_export(const bass_state* st, uint64_t* ok, double* oa, int key_bits, const WsView& ws,
-                       bass_ctrl* ctrl, cudaStream_t s) {
-  KLAUNCH(S_SORT, s, k_export<<<device().grid_small, 256, 0, s>>>(st, ok, reinterpret_cast<double2*>(oa), ws.max_n));
-  return run_radix_sort(ok, reinterpret_cast<double2*>(oa), 0, reinterpret_cast<const long long*>(&st->nnz), key_bits, ws, ctrl, s);
+                       bass_ctrl* ctrl, cudaStream_t s, int amp_type) {
+  KLAUNCH(S_SORT, s, k_export<<<device().grid_small, 256, 0, s>>>(st, ok, oa, ws.max_n, amp_type, ctrl));
+  return run_radix_sort(ok, oa, 0, reinterpret_cast<const long long*>(&st->nnz), key_bits, ws, ctrl, s,
+                        amp_type == BASS_AMP_C64);
 }
 
 cudaError_t run_merge_sorted(uint64_t* keys, double* amps, long long n, long long* n_out,
                              const WsView& ws, bass_ctrl* ctrl, cudaStream_t s) {
   cudaError_t e = zero_small(ws, s);
   if (e != cudaSuccess) return e;
-  KLAUNCH(S_MERGE_RUNS, s, k_merge_runs<<<device().grid_small, 256, 0, s>>>(keys, reinterpret_cast<double2*>(amps), nullptr, n, ws,
-                                                   ctrl));
-  KLAUNCH(S_MERGE_RUNS, s, k_merge_out<<<device().grid_small, 256, 0, s>>>(keys, reinterpret_cast<double2*>(amps), ws, n_out, nullptr));
+  KLAUNCH(S_MERGE_RUNS, s, k_merge_runs<<<device().grid_small, 256, 0, s>>>(keys, amps, nullptr, n, ws, ctrl, 0));
+  KLAUNCH(S_MERGE_RUNS, s, k_merge_out<<<device().grid_small, 256, 0, s>>>(keys, amps, ws, n_out, nullptr, 0));
   return cudaGetLastError();
 }
 

@@ -18,9 +18,12 @@ from .linalg import is_gate_diagonal  # noqa: F401  (re-exported for callers)
 class SparseState:
     """|phi> = sum_i alpha_i |x_i>, at most ``k`` entries after a truncation."""
 
-    def __init__(self, num_qubits, k, init_state=None, *, _capacity=None, _engine=None, _trace_cap=0):
+    def __init__(self, num_qubits, k, init_state=None, *, dtype=np.complex128, _capacity=None, _engine=None,
+                 _trace_cap=0):
         self.N = int(num_qubits)
         self.k = int(k)
+        self.dtype = np.dtype(dtype)
+        at = nat.amp_type_of(self.dtype)
         self.RADIX_THRESHOLD = 2000  # kept for interface parity; the GPU path always merges
         # like the reference's 4k temporary buffers: a gate whose truncation is
         # decided afterwards (random-k) first writes up to 4k entries
@@ -28,9 +31,9 @@ class SparseState:
         self._eng = _engine if _engine is not None else nat.Engine(
             max_n=4 * cap + 64, num_qubits=self.N, trace_cap=_trace_cap)
         key = 0 if init_state is None else int(init_state)
-        self._cur = nat.DevState(self._eng, cap, key)
-        self._tmp = nat.DevState(self._eng, cap)
-        self._tmp2 = nat.DevState(self._eng, cap)
+        self._cur = nat.DevState(self._eng, cap, key, at)
+        self._tmp = nat.DevState(self._eng, cap, 0, at)
+        self._tmp2 = nat.DevState(self._eng, cap, 0, at)
         self._version = 0
         self._export = None
 
@@ -76,7 +79,7 @@ class SparseState:
         self._touch()
 
     def copy(self):
-        new = SparseState(self.N, self.k, _capacity=self._cur.cap)
+        new = SparseState(self.N, self.k, dtype=self.dtype, _capacity=self._cur.cap)
         x, a = self._exported()
         new.load(x, a)
         new.gamma = self.gamma
@@ -86,7 +89,7 @@ class SparseState:
         if self.N > 20:
             raise ValueError("Dense conversion only allowed for N <= 20")
         x, a = self._exported()
-        dense = np.zeros(2 ** self.N, dtype=np.complex128)
+        dense = np.zeros(2 ** self.N, dtype=self.dtype)
         dense[x.astype(np.int64)] = a
         return dense
 
@@ -172,7 +175,7 @@ class SparseState:
     def _spare(self):
         """A fourth device buffer (the 2-qubit passes park the saved state there)."""
         if getattr(self, "_tmp3", None) is None:
-            self._tmp3 = nat.DevState(self._eng, self._cur.cap)
+            self._tmp3 = nat.DevState(self._eng, self._cur.cap, 0, self._cur.amp_type)
         return self._tmp3
 
     def _phase_2q(self, diag, q1, q2):

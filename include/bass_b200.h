@@ -22,7 +22,10 @@
  * pointing at two caller-owned arrays of capacity cap: keys (uint64) and amps
  * (complex128, interleaved re/im).  Keys are stored in a permuted bit order:
  * physical bit p holds qubit qat[p] (pos[] is the inverse), and the array is
- * sorted ascending by physical key with no duplicates.  Every pairing kernel
+ * sorted ascending by physical key with no duplicates.  A state stores
+ * complex128 or complex64 amplitudes (amp_type); every entry point reads the
+ * type from the descriptor, except the few whose host arrays must have it
+ * (the _typed set-up, import and export calls).  Every pairing kernel
  * moves the qubits it acts on to the lowest physical bits, so a gate's
  * partners always meet in one merge pass.  A stored amplitude is multiplied
  * by rscale[0] and then by rscale[1] on every read: a renormalisation is
@@ -49,6 +52,14 @@ extern "C" {
 
 #define BASS_MAX_QUBITS 63
 
+/* amplitude storage of a state (bass_state.amp_type) */
+#define BASS_AMP_C128 0 /* complex128: interleaved double re, im                 */
+#define BASS_AMP_C64 1  /* complex64: interleaved float re, im (amps points at
+                           floats); gate arithmetic in FP32 with compensated
+                           (error-free) products and sums, while |a|^2, every
+                           sum, the top-k threshold and the RDM moments stay in
+                           FP64 */
+
 /* ---- device-resident descriptors (layout is part of the ABI) ------------- */
 typedef struct bass_state {
   uint64_t* keys;     /* physical keys, sorted ascending, unique            */
@@ -57,7 +68,7 @@ typedef struct bass_state {
   int64_t cap;        /* capacity of keys/amps                               */
   double rscale[2];   /* pending renormalisation factors (1.0 = none)        */
   int32_t nq;         /* number of qubits                                    */
-  int32_t pad0;
+  int32_t amp_type;   /* BASS_AMP_C128 or BASS_AMP_C64 (storage of amps)     */
   int8_t pos[64];     /* pos[q]: physical bit of qubit q                     */
   int8_t qat[64];     /* qat[p]: qubit stored at physical bit p              */
 } bass_state;
@@ -129,12 +140,22 @@ size_t bass_workspace_bytes(int64_t max_in, int64_t max_out, int num_qubits);
 /* SparseState.__init__ (sparse_state.py:202-219): |init_key>, amplitude 1. */
 int bass_state_init(bass_state* st, uint64_t* keys, double* amps, int64_t cap, int num_qubits,
                     uint64_t init_key, void* stream);
+/* bass_state_init for a state of the given amplitude storage (BASS_AMP_*);
+   amps then holds cap complex values of that type. */
+int bass_state_init_typed(bass_state* st, uint64_t* keys, double* amps, int64_t cap, int num_qubits,
+                          uint64_t init_key, int amp_type, void* stream);
 /* Build a state in the buffers (st_keys, st_amps, capacity cap) from n
    entries (true keys, amps) in any order: radix sort by key, then duplicates
    are merged as sparse_state.py:127-147 does; identity bit order. */
 int bass_state_import_into(bass_state* st, uint64_t* st_keys, double* st_amps, int64_t cap,
                            const uint64_t* keys, const double* amps, int64_t n, int num_qubits,
                            void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream);
+/* bass_state_import_into for a state of the given amplitude storage: amps
+   and st_amps hold values of that type; duplicates of complex64 states are
+   summed in FP32 with the compensated (TwoSum) sum. */
+int bass_state_import_typed(bass_state* st, uint64_t* st_keys, double* st_amps, int64_t cap,
+                            const uint64_t* keys, const double* amps, int64_t n, int num_qubits, int amp_type,
+                            void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream);
 /* Write the state as true keys sorted ascending and amplitudes with the
    pending renormalisation applied (SparseState.x / .alpha); st->nnz entries.
    _bits sorts on the low key_bits bits only (keys < 2^num_qubits). */
@@ -142,6 +163,11 @@ int bass_state_export(const bass_state* st, uint64_t* out_keys, double* out_amps
                       size_t ws_bytes, bass_ctrl* ctrl, void* stream);
 int bass_state_export_bits(const bass_state* st, uint64_t* out_keys, double* out_amps, int key_bits,
                            void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream);
+/* bass_state_export_bits for a state of the given amplitude storage (out_amps
+   holds values of that type); a state of another type is refused on the
+   device (BASS_ERR_ARG in ctrl, nothing written). */
+int bass_state_export_typed(const bass_state* st, uint64_t* out_keys, double* out_amps, int key_bits,
+                            int amp_type, void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream);
 /* Copy descriptor contents (pointers included) from src to dst. */
 int bass_state_copy_desc(bass_state* dst, const bass_state* src, void* stream);
 /* Deep copy of entries into dst's own buffers (SparseState.copy). */
