@@ -4,6 +4,7 @@
 
 #include <atomic>
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "internal.h"
@@ -143,6 +144,26 @@ bool carve(void* ws, size_t ws_bytes, WsView* v) {
 
 static int status_of(cudaError_t e) { return e == cudaSuccess ? BASS_OK : BASS_ERR_CUDA; }
 
+// The amplitude type of every descriptor set up through this library, keyed
+// by its device address (unique across devices under unified addressing).
+// Launches pick the kernels for that type from here; the kernels compare it
+// with the descriptor's own amp_type and refuse a mismatch (BASS_ERR_ARG).
+// A descriptor never set up here counts as complex128.
+static std::mutex g_type_mu;
+static std::unordered_map<const void*, int> g_types;
+
+static void remember_type(const bass_state* st, int amp_type) {
+  std::lock_guard<std::mutex> lk(g_type_mu);
+  if (amp_type == BASS_AMP_C128) g_types.erase(st);
+  else g_types[st] = amp_type;
+}
+
+int state_c64(const bass_state* st) {
+  std::lock_guard<std::mutex> lk(g_type_mu);
+  const auto it = g_types.find(st);
+  return it != g_types.end() && it->second == BASS_AMP_C64;
+}
+
 static void load_G(OpArgs& a, const double* g, int n) {
   for (int i = 0; i < n; ++i) a.G[i] = make_double2(g[2 * i], g[2 * i + 1]);
 }
@@ -175,6 +196,7 @@ int bass_state_init_typed(bass_state* st, uint64_t* keys, double* amps, int64_t 
   if (!st || !keys || !amps || cap < 1 || num_qubits < 1 || num_qubits > BASS_MAX_QUBITS || !amp_type_ok(amp_type))
     return BASS_ERR_ARG;
   if (num_qubits < 64 && (init_key >> num_qubits) != 0) return BASS_ERR_ARG;
+  remember_type(st, amp_type);
   return status_of(run_state_init(st, keys, amps, cap, num_qubits, init_key, amp_type, (cudaStream_t)stream));
 }
 
@@ -191,6 +213,7 @@ int bass_state_import_typed(bass_state* st, uint64_t* st_keys, double* st_amps, 
     return BASS_ERR_ARG;
   CHECK_WS(ws, ws_bytes, v);
   if (n > v.max_n) return BASS_ERR_WORKSPACE;
+  remember_type(st, amp_type);
   return status_of(run_import(st, keys, amps, n, num_qubits, v, ctrl, (cudaStream_t)stream, st_keys,
                               st_amps, cap, amp_type));
 }
@@ -222,6 +245,7 @@ int bass_state_export_bits(const bass_state* st, uint64_t* out_keys, double* out
 
 int bass_state_copy_desc(bass_state* dst, const bass_state* src, void* stream) {
   if (!dst || !src) return BASS_ERR_ARG;
+  remember_type(dst, state_c64(src) ? BASS_AMP_C64 : BASS_AMP_C128);
   return status_of(run_copy_desc(dst, src, (cudaStream_t)stream));
 }
 
@@ -241,7 +265,7 @@ int bass_gate_1q(const bass_state* in, bass_state* out, const double* host_G, in
   CHECK_WS(ws, ws_bytes, v);
   cudaStream_t s = (cudaStream_t)stream;
   OpArgs a{};
-  a.in = in; a.out = out; a.ctrl = ctrl; a.ws = v; a.q = q; a.gb = 0;
+  a.in = in; a.out = out; a.ctrl = ctrl; a.ws = v; a.q = q; a.gb = 0; a.c64 = state_c64(in);
   load_G(a, host_G, 4);
   cudaError_t e = run_merge_op(K_GATE1, a, tr, 0, 0, s);
   if (e == cudaSuccess && tr.trace) e = run_fingerprint(out, kSigPmin, nullptr, v, s, ctrl, 1, 1);
@@ -257,14 +281,14 @@ int bass_gate_2q(const bass_state* in, bass_state* tmp, bass_state* out, const d
   cudaStream_t s = (cudaStream_t)stream;
   // pass 1: bring q2 to the lowest physical bit (a pure reorder)
   OpArgs a{};
-  a.in = in; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = q2; a.gb = 0;
+  a.in = in; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = q2; a.gb = 0; a.c64 = state_c64(in);
   bass_trunc none{};
   none.k_cond = -1;
   cudaError_t e = run_merge_op(K_PERM, a, none, 0, 0, s);
   if (e != cudaSuccess) return status_of(e);
   // pass 2: merge on q1 above it; groups of four are (b_q1, b_q2) in input-index order
   OpArgs b{};
-  b.in = tmp; b.out = out; b.ctrl = ctrl; b.ws = v; b.q = q1; b.gb = 1;
+  b.in = tmp; b.out = out; b.ctrl = ctrl; b.ws = v; b.q = q1; b.gb = 1; b.c64 = a.c64;
   load_G(b, host_G, 16);
   e = run_merge_op(K_GATE2, b, tr, 0, 0, s);
   if (e == cudaSuccess && tr.trace) e = run_fingerprint(out, kSigPmin, nullptr, v, s, ctrl, 1, 1);
@@ -280,14 +304,14 @@ int bass_rotate_2q(const bass_state* in, bass_state* tmp, bass_state* out, const
   cudaStream_t s = (cudaStream_t)stream;
   // pass 1: bring q2 to the lowest physical bit (a pure reorder)
   OpArgs a{};
-  a.in = in; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = q2; a.gb = 0;
+  a.in = in; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = q2; a.gb = 0; a.c64 = state_c64(in);
   bass_trunc none{};
   none.k_cond = -1;
   cudaError_t e = run_merge_op(K_PERM, a, none, 0, 0, s);
   if (e != cudaSuccess) return status_of(e);
   // pass 2: groups of four (b_q1, b_q2), the rotation's drop rule
   OpArgs b{};
-  b.in = tmp; b.out = out; b.ctrl = ctrl; b.ws = v; b.q = q1; b.gb = 1; b.drop_zero = 2;
+  b.in = tmp; b.out = out; b.ctrl = ctrl; b.ws = v; b.q = q1; b.gb = 1; b.drop_zero = 2; b.c64 = a.c64;
   load_G(b, host_U4, 16);
   e = run_merge_op(K_GATE2, b, tr, 0, 0, s);
   if (e == cudaSuccess && tr.trace) e = run_fingerprint(out, kSigPmin, nullptr, v, s, ctrl, 1, 1);
@@ -300,7 +324,7 @@ int bass_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* r
       q2 >= BASS_MAX_QUBITS || q1 == q2)
     return BASS_ERR_ARG;
   CHECK_WS(ws, ws_bytes, v);
-  return status_of(run_rdm_2q(st, tmp, q1, q2, rho, ctrl, v, (cudaStream_t)stream));
+  return status_of(run_rdm_2q(st, tmp, q1, q2, rho, ctrl, v, (cudaStream_t)stream, state_c64(st)));
 }
 
 int bass_to_dense(const bass_state* st, const double* host_U, int nq, double* psi, bass_ctrl* ctrl, void* stream) {
@@ -333,7 +357,7 @@ int bass_phase_1q(bass_state* st, bass_state* tmp, const double* host_diag2, int
                   void* ws, size_t ws_bytes, void* stream) {
   if (!st || !tmp || st == tmp || !host_diag2 || q < 0 || q >= BASS_MAX_QUBITS || !ctrl) return BASS_ERR_ARG;
   CHECK_WS(ws, ws_bytes, v);
-  return status_of(run_phase1q(st, tmp, host_diag2, q, ctrl, v, (cudaStream_t)stream));
+  return status_of(run_phase1q(st, tmp, host_diag2, q, ctrl, v, (cudaStream_t)stream, state_c64(st)));
 }
 
 int bass_phase_2q(bass_state* st, const double* host_diag4, int q1, int q2, bass_ctrl* ctrl, void* stream) {
@@ -349,7 +373,7 @@ int bass_topk(const bass_state* in, bass_state* out, bass_trunc tr, bass_ctrl* c
   CHECK_WS(ws, ws_bytes, v);
   cudaStream_t s = (cudaStream_t)stream;
   OpArgs a{};
-  a.in = in; a.out = out; a.ctrl = ctrl; a.ws = v; a.q = 0; a.gb = 0;
+  a.in = in; a.out = out; a.ctrl = ctrl; a.ws = v; a.q = 0; a.gb = 0; a.c64 = state_c64(in);
   cudaError_t e = run_merge_op(K_IDENT, a, tr, 0, 0, s);
   if (e == cudaSuccess && tr.trace) e = run_fingerprint(out, kSigPmin, nullptr, v, s, ctrl, 1, 1);
   return status_of(e);
@@ -403,7 +427,7 @@ int bass_rdm_1q(const bass_state* st, int num_qubits, double* rho, bass_ctrl* ct
                 size_t ws_bytes, void* stream) {
   if (!st || !rho || !ctrl || num_qubits < 1 || num_qubits > BASS_MAX_QUBITS) return BASS_ERR_ARG;
   CHECK_WS(ws, ws_bytes, v);
-  return status_of(run_rdm(st, num_qubits, rho, ctrl, v, (cudaStream_t)stream));
+  return status_of(run_rdm(st, num_qubits, rho, ctrl, v, (cudaStream_t)stream, state_c64(st)));
 }
 
 int bass_rotate_step(bass_state* cur, bass_state* tmp, const double* host_U, int j, int64_t k, int trace,
@@ -412,7 +436,7 @@ int bass_rotate_step(bass_state* cur, bass_state* tmp, const double* host_U, int
   CHECK_WS(ws, ws_bytes, v);
   cudaStream_t s = (cudaStream_t)stream;
   OpArgs a{};
-  a.in = cur; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = j; a.gb = 0;
+  a.in = cur; a.out = tmp; a.ctrl = ctrl; a.ws = v; a.q = j; a.gb = 0; a.c64 = state_c64(cur);
   load_G(a, host_U, 4);
   bass_trunc tr{};
   tr.k_cond = k;

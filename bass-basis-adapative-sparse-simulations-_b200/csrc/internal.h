@@ -33,6 +33,9 @@ struct OpArgs {
   int j;          // rotation step: the rotated qubit
   long long k_cond, k_keep;
   bass_trunc tr;  // finalize_op: gamma / renormalisation rules
+  int c64;        // the input state stores complex64 amplitudes (selects the kernels)
+  int pad;
+  double* rho;    // RDM moments of a segmented RDM (4 per qubit)
 };
 
 enum Slot {
@@ -87,22 +90,26 @@ struct Device {
 const Device& device();
 
 bool carve(void* ws, size_t ws_bytes, WsView* v);
+// 1 if the state was set up (bass_state_init_typed / import / copy_desc) with
+// complex64 amplitudes: the host's record of each descriptor's type, which
+// selects the kernels to launch (the kernels check the descriptor's own field)
+int state_c64(const bass_state* st);
 size_t ws_bytes_for(long long max_n);
 
 // merge.cu
 cudaError_t run_merge_op(int kind, OpArgs a, const bass_trunc& tr, int finalize_mode, int j,
                          cudaStream_t s);
 cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
-                    cudaStream_t s);
+                    cudaStream_t s, int c64);
 cudaError_t zero_small(const WsView& ws, cudaStream_t s);
 cudaError_t run_to_dense(const bass_state* st, const double* host_U, int nq, double* psi, bass_ctrl* ctrl,
                          cudaStream_t s);
 cudaError_t run_dot(const double* u, const double* v, long long n, const bass_state* st, int nq, double* out,
                     bass_ctrl* ctrl, const WsView& ws, cudaStream_t s);
 cudaError_t run_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* rho, bass_ctrl* ctrl,
-                       const WsView& ws, cudaStream_t s);
+                       const WsView& ws, cudaStream_t s, int c64);
 cudaError_t run_rdm_prepared(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
-                             cudaStream_t s);
+                             cudaStream_t s, int c64);
 cudaError_t run_ident_write(OpArgs a, cudaStream_t s);
 // rotation step: keep the candidate in *tmp if the decision accepted it
 cudaError_t run_commit(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const WsView& ws, int j, int trace,
@@ -122,7 +129,7 @@ cudaError_t run_radix_sort(uint64_t* keys, double* amps, long long n, const long
 cudaError_t run_renorm(bass_state* st, bass_ctrl* ctrl, const WsView& ws, cudaStream_t s);
 cudaError_t run_phase2q(bass_state* st, const double* d, int q1, int q2, bass_ctrl* ctrl, cudaStream_t s);
 cudaError_t run_phase1q(bass_state* st, bass_state* tmp, const double* g, int q, bass_ctrl* ctrl,
-                        const WsView& ws, cudaStream_t s);
+                        const WsView& ws, cudaStream_t s, int c64);
 cudaError_t run_state_init(bass_state* st, uint64_t* keys, double* amps, long long cap, int nq,
                            uint64_t key, int amp_type, cudaStream_t s);
 cudaError_t run_import(bass_state* st, const uint64_t* keys, const double* amps, long long n, int nq,

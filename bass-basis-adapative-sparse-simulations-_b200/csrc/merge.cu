@@ -47,6 +47,15 @@ struct Hdr {
   int8_t qat_out[64];
 };
 
+// The blocks of a launch that work on one op.  A plain launch is one group
+// (blockIdx.x of gridDim.x); a segmented launch (one op on each of many
+// states) splits its grid into one group per state, see seg_enter.
+struct Grp {
+  int bid;   // block index within the group
+  int nblk;  // blocks in the group
+};
+__device__ __forceinline__ Grp whole_grid() { return Grp{(int)blockIdx.x, (int)gridDim.x}; }
+
 // The op's output qubit order: the input's, with the target qubit's
 // position t = pos[q] moved down to gb (positions gb..t-1 move up by one) for
 // the kinds that bring a target to the low bits.  One position per thread
@@ -70,16 +79,18 @@ __device__ __forceinline__ void out_order_par(const bass_state* in, int kind, in
 // record per boundary: P' (adjusted Z position), s, mid, e (block bounds), i, j
 // zero: also clear the op's small workspace region (what zero_small clears);
 // nothing here reads it, and the kernels after the partition find it zeroed.
-__global__ void k_partition(const __grid_constant__ OpArgs a, int kind, int zero) {
-  pdl_wait();
-  const int set = blockIdx.y;
-  if (zero && set == 0) {
-    unsigned long long* zp = reinterpret_cast<unsigned long long*>(a.ws.counters);
-    const long long nw =
-        (long long)((reinterpret_cast<const char*>(a.ws.status + a.ws.max_tiles) - reinterpret_cast<const char*>(zp)) / 8);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x)
-      zp[i] = 0ULL;
-  }
+// The op's small workspace region (tile counters, histograms, selection
+// state, look-back status words: what zero_small clears), zeroed by a group.
+__device__ __forceinline__ void zero_op_region(const OpArgs& a, Grp g) {
+  unsigned long long* zp = reinterpret_cast<unsigned long long*>(a.ws.counters);
+  const long long nw =
+      (long long)((reinterpret_cast<const char*>(a.ws.status + a.ws.max_tiles) - reinterpret_cast<const char*>(zp)) / 8);
+  for (long long i = (long long)g.bid * blockDim.x + threadIdx.x; i < nw; i += (long long)g.nblk * blockDim.x)
+    zp[i] = 0ULL;
+}
+
+__device__ __forceinline__ void partition_body(const OpArgs& a, int kind, int zero, int set, Grp g) {
+  if (zero && set == 0) zero_op_region(a, g);
   const bass_state* in = a.in;
   const long long n = in->nnz;
   const int q = (kind == K_RDM) ? set : a.q;
@@ -90,8 +101,8 @@ __global__ void k_partition(const __grid_constant__ OpArgs a, int kind, int zero
   const long long ntiles = merge_tiles(n);
   long long* recs = a.ws.part + (long long)set * (a.ws.max_tiles + 1) * 6;
   const int lane = threadIdx.x & 31;
-  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const long long warp = ((long long)g.bid * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)g.nblk * blockDim.x) >> 5;
   if (ntiles + 1 > a.ws.max_tiles + 1) {
     if (warp == 0 && lane == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
     return;
@@ -151,6 +162,11 @@ __global__ void k_partition(const __grid_constant__ OpArgs a, int kind, int zero
     }
   }
   pdl_trigger();
+}
+
+__global__ void k_partition(const __grid_constant__ OpArgs a, int kind, int zero) {
+  pdl_wait();
+  partition_body(a, kind, zero, blockIdx.y, whole_grid());
 }
 
 // ---------------------------------------------------------------------------
@@ -414,14 +430,14 @@ __device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int
 // Block-wide, at the end of a write pass: the last CTA to arrive writes the
 // output descriptor (its qubit order one position per thread, the rest by
 // finalize_op).
-__device__ void write_done(const OpArgs& a, int kind) {
+__device__ void write_done(const OpArgs& a, int kind, Grp g) {
   __shared__ int sLastW;
   __shared__ int8_t sQo[64];
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned long long d = atomicAdd(&reinterpret_cast<unsigned long long*>(a.ws.counters)[59], 1ULL);
-    sLastW = (d == gridDim.x - 1);
+    sLastW = (d == (unsigned long long)g.nblk - 1);
   }
   __syncthreads();
   if (!sLastW) return;
@@ -480,9 +496,8 @@ __device__ __forceinline__ void load_sel(SelState* dst, const SelState* src) {
 // the child count), P_WRITE (the first pass of a 2-qubit gate, one child per
 // entry, and the compaction after a diagonal 1-qubit gate), P_RDM (per-qubit
 // moments).
-template <int KIND, int PASS>
-__global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ OpArgs a) {
-  pdl_wait();
+template <int KIND, int PASS, bool C64>
+__device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
   extern __shared__ __align__(16) unsigned char smem[];
   double2* sA = reinterpret_cast<double2*>(smem);
   uint64_t* sZ = reinterpret_cast<uint64_t*>(sA + kTilePad);
@@ -514,6 +529,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
     H.r1 = in->rscale[1];
     H.nq = in->nq;
     H.c64 = in->amp_type == BASS_AMP_C64;
+    if (H.c64 != (int)C64) set_error(a.ctrl, BASS_ERR_ARG);  // launched for the other amplitude type
     H.t = (KIND == K_IDENT || KIND == K_RDM) ? 0 : in->pos[a.q];
     H.ntiles = (KIND == K_IDENT) ? plain_tiles(H.n) : merge_tiles(H.n);
   }
@@ -523,8 +539,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
   const int gb = a.gb;
   const long long ntiles = H.ntiles;
   constexpr int NS = slots_per_entry(KIND);
-  const bool bad = ntiles > a.ws.max_tiles || (PASS == P_HIST && (long long)NS * H.n > a.ws.max_n);
-  if (bad && blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+  const bool bad = ntiles > a.ws.max_tiles || (PASS == P_HIST && (long long)NS * H.n > a.ws.max_n) ||
+                   H.c64 != (int)C64;
+  if (bad && g.bid == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
   if (bad && PASS != P_WRITE) return;
   const bool scaled = !(H.r0 == 1.0 && H.r1 == 1.0);
   // P_RDM: items are (set, tile); K_RDM sets are qubits, the 4x4 moments of
@@ -593,7 +610,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
       const int o1 = (int)sSegOff[1], o2 = (int)sSegOff[2], o3 = (int)sSegOff[3], o4 = (int)sSegOff[4];
       const unsigned zb = (unsigned)__cvta_generic_to_shared(sZ);
       const unsigned ab = (unsigned)__cvta_generic_to_shared(sA);
-      const bool c64 = H.c64;
+      constexpr bool c64 = C64;
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
         const int e = k * kThreads + tid;
@@ -699,7 +716,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
       __syncthreads();
     }
 
-    const bool c64 = H.c64 != 0;
+    constexpr bool c64 = C64;
     const AmpView amp{sA, reinterpret_cast<const float2*>(sA), KIND == K_IDENT ? nullptr : sPerm, H.r0, H.r1,
                       scaled, c64};
 
@@ -917,7 +934,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
 
   pdl_trigger();
   // ---- write pass: the last CTA to finish writes the output descriptor ------
-  if (PASS == P_WRITE && a.fin) write_done(a, KIND);
+  if (PASS == P_WRITE && a.fin) write_done(a, KIND, g);
 
   // ---- flush: the CTA's child count ----------------------------------------
   if (PASS == P_HIST) {
@@ -928,9 +945,16 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
     if (tid == 0) {
       long long c = 0;
       for (int w = 0; w < kThreads / 32; ++w) c += reinterpret_cast<long long*>(sRed)[w];
-      a.ws.partials[blockIdx.x].c[0] = c;
+      a.ws.partials[g.bid].c[0] = c;
     }
   }
+}
+
+// The tile pass of one op on a state of complex64 (C64) or complex128 amplitudes.
+template <int KIND, int PASS, bool C64>
+__global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ OpArgs a) {
+  pdl_wait();
+  tile_body<KIND, PASS, C64>(a, whole_grid());
 }
 
 // ---------------------------------------------------------------------------
@@ -963,7 +987,7 @@ constexpr int kSelThreads = 512;
 
 // Grid-wide barrier of the selection's grid (every block resident, see
 // launch_select_t).  Returns false (error recorded) if the wait gave up.
-__device__ bool grid_sync(const OpArgs& a) {
+__device__ bool grid_sync(const OpArgs& a, Grp gr) {
   __shared__ int sOk;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -975,7 +999,7 @@ __device__ bool grid_sync(const OpArgs& a) {
     __threadfence();
     const unsigned long long arrived = atomicAdd(cnt, 1ULL);
     int ok = 1;
-    if (arrived == gridDim.x - 1) {
+    if (arrived == (unsigned long long)gr.nblk - 1) {
       atomicExch(cnt, 0ULL);
       __threadfence();
       st_release(gen, g + 1);
@@ -1063,15 +1087,15 @@ __device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, 
 // 37-49 of the slots whose bits >> 50 equal pre), added into gh.
 template <int LEVEL>
 __device__ void slot_hist_phase(const unsigned long long* slots, long long nslots, unsigned long long pre,
-                                unsigned int* h, unsigned int* gh) {
+                                unsigned int* h, unsigned int* gh, Grp g) {
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) h[i] = 0;
   __syncthreads();
   // eight slots per thread and round, plain shared atomics (measured faster
   // here than warp aggregation with __match_any_sync)
   const ulonglong2* v = reinterpret_cast<const ulonglong2*>(slots);
   const long long n2 = nslots >> 1;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long b = (long long)blockIdx.x * blockDim.x; b < n2; b += 4 * stride) {
+  const long long stride = (long long)g.nblk * blockDim.x;
+  for (long long b = (long long)g.bid * blockDim.x; b < n2; b += 4 * stride) {
     unsigned key[8];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -1090,7 +1114,7 @@ __device__ void slot_hist_phase(const unsigned long long* slots, long long nslot
     for (int u = 0; u < 8; ++u)
       if (key[u] != 0xFFFFFFFFu) atomicAdd(&h[key[u]], 1u);
   }
-  if ((nslots & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+  if ((nslots & 1) && g.bid == 0 && threadIdx.x == 0) {
     const unsigned long long bits = slots[nslots - 1];
     const bool valid = bits != ~0ULL && (LEVEL == 1 || (bits >> 50) == pre);
     const unsigned bin = LEVEL == 1 ? (unsigned)(bits >> 50) : (unsigned)((bits >> 37) & (kHistBins - 1));
@@ -1280,7 +1304,7 @@ __device__ __forceinline__ long long tile_of(long long z, int kind, const long l
 // cpre, all below T) are collected for settle_small / settle_radix as well.
 template <bool P2>
 __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long long T, bool incl, bool trunc,
-                            i128* sRed, bool cand, unsigned long long cpre, const int8_t* qat) {
+                            i128* sRed, bool cand, unsigned long long cpre, const int8_t* qat, Grp g) {
   const long long n = a.in->nnz;
   const long long nslots = (long long)ns * n;
   const bool sums = P2 || trunc;
@@ -1291,8 +1315,8 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
   const long long* part = a.ws.part;
   i128 v[3] = {0, 0, 0};
   const long long nchunk = (nslots + 7) >> 3;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long cb = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); cb < nchunk; cb += stride) {
+  const long long stride = (long long)g.nblk * blockDim.x;
+  for (long long cb = (long long)g.bid * blockDim.x + (threadIdx.x & ~31); cb < nchunk; cb += stride) {
     const long long c = cb + lane;  // this thread's chunk: slots [8c, 8c + 8)
     const long long s0 = c << 3;
     unsigned long long x[8];
@@ -1400,7 +1424,7 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
   }
   block_sum_i128<3>(v, sRed);
   if (threadIdx.x == 0) {
-    Partial* pt = a.ws.partials + blockIdx.x;
+    Partial* pt = a.ws.partials + g.bid;
     pt->s[0] = v[0];
     pt->s[1] = v[1];
     pt->s[2] = v[2];
@@ -1488,24 +1512,22 @@ __device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j
 
 // After count_phase: the last block to finish runs final_phase (the others
 // exit), which needs every block's partial sums and tile counts.
-__device__ void finish_by_last_block(const OpArgs& a, int kind, int mode, int j, int trace, i128* sRed) {
+__device__ void finish_by_last_block(const OpArgs& a, int kind, int mode, int j, int trace, i128* sRed, Grp g) {
   __shared__ int sLast;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned long long d = atomicAdd(&reinterpret_cast<unsigned long long*>(a.ws.counters)[58], 1ULL);
-    sLast = (d == gridDim.x - 1);
+    sLast = (d == (unsigned long long)g.nblk - 1);
     __threadfence();
   }
   __syncthreads();
-  if (sLast) final_phase(a, gridDim.x, kind, mode, j, trace, sRed);
+  if (sLast) final_phase(a, g.nblk, kind, mode, j, trace, sRed);
 }
 
-// nblk_hist: CTAs of the evaluation pass (per-CTA child counts in partials c[0]).
 template <bool P2>
-__global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_constant__ OpArgs a, int ns, int kind, int nblk_hist, int mode,
-                                                              int j, int trace) {
-  pdl_wait();
+__device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int kind, int nblk_hist, int mode, int j,
+                                            int trace) {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned int* h = reinterpret_cast<unsigned int*>(smem);
   __shared__ long long sS[kSelThreads / 32];
@@ -1517,7 +1539,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
   const long long nslots = (long long)ns * n;
   const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
   if (nslots > a.ws.max_n || ntiles > a.ws.max_tiles || n >= (1LL << 31)) {  // uniform: every block returns
-    if (blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+    if (g.bid == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
     return;
   }
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
@@ -1547,16 +1569,16 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
     incl = false;
   } else if (trunc) {
     // 2. radix select on the bit patterns
-    slot_hist_phase<1>(slots, nslots, 0, h, a.ws.hist1);
-    if (!grid_sync(a)) return;
+    slot_hist_phase<1>(slots, nslots, 0, h, a.ws.hist1, g);
+    if (!grid_sync(a, g)) return;
     long long c_gt, c_b1;
     const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, &c_b1);
     const long long need = a.k_keep - c_gt;
     if (c_b1 == need) {
       T = (unsigned long long)b1 << 50;
     } else {
-      slot_hist_phase<2>(slots, nslots, (unsigned long long)b1, h, a.ws.hist2);
-      if (!grid_sync(a)) return;
+      slot_hist_phase<2>(slots, nslots, (unsigned long long)b1, h, a.ws.hist2, g);
+      if (!grid_sync(a, g)) return;
       long long c_gt2, c_b2;
       const int b2 = find_bin(a.ws.hist2, need, &c_gt2, &c_b2);
       const long long need2 = need - c_gt2;
@@ -1573,7 +1595,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
       }
     }
   }
-  if (blockIdx.x == 0 && tid == 0) {
+  if (g.bid == 0 && tid == 0) {
     sel->n_out = n_out;
     sel->k_keep = a.k_keep;
     sel->do_trunc = trunc ? 1 : 0;
@@ -1585,35 +1607,35 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
   if (late) {
     out_order_par(a.in, kind, a.q, a.gb, sQat);
     __syncthreads();
-    if (blockIdx.x == 0 && tid < 64) sel->qat[tid] = sQat[tid];
+    if (g.bid == 0 && tid < 64) sel->qat[tid] = sQat[tid];
   }
   // 3. survivors per tile and exact sums
-  count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, late, lpre, sQat);
+  count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, late, lpre, sQat, g);
   if (late) {
     // 3b. the boundary bin: its threshold pair, then its survivors counted
     // per tile and their mass added to this block's partial sums
-    if (!grid_sync(a)) return;
+    if (!grid_sync(a, g)) return;
     __shared__ long long sM;
     __shared__ unsigned long long sTb, sTk;
     if (tid == 0) sM = *(volatile long long*)&sel->n_cand;
     __syncthreads();
     long long m = sM;
     if (m > a.ws.max_n) {
-      if (blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+      if (g.bid == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
       m = a.ws.max_n;
     }
     unsigned long long tb, tk;
     if (m <= kCandSmem) {
       settle_small(a, smem, m, lneed, &tb, &tk);
     } else {
-      if (blockIdx.x == 0) {
+      if (g.bid == 0) {
         settle_radix(a, smem, m, lneed, lpre, &tb, &tk);
         if (tid == 0) {
           sel->t_bits = tb;
           sel->t_key = tk;
         }
       }
-      if (!grid_sync(a)) return;
+      if (!grid_sync(a, g)) return;
       if (tid == 0) {
         sTb = *(volatile unsigned long long*)&sel->t_bits;
         sTk = *(volatile unsigned long long*)&sel->t_key;
@@ -1622,13 +1644,13 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
       tb = sTb;
       tk = sTk;
     }
-    if (blockIdx.x == 0 && tid == 0) {
+    if (g.bid == 0 && tid == 0) {
       sel->t_bits = tb;
       sel->t_key = tk;
     }
     const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;
     i128 v[3] = {0, 0, 0};
-    for (long long k = (long long)blockIdx.x * blockDim.x + tid; k < m; k += (long long)gridDim.x * blockDim.x) {
+    for (long long k = (long long)g.bid * blockDim.x + tid; k < m; k += (long long)g.nblk * blockDim.x) {
       const unsigned long long i = __ldcg(a.ws.cand_bits + k);
       const unsigned long long bits = __ldcg(slots + i);
       if (bits > tb || (bits == tb && __ldcg(a.ws.cand_key + k) <= tk)) {
@@ -1643,14 +1665,22 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
     }
     block_sum_i128<3>(v, sRed);
     if (tid == 0) {
-      Partial* pt = a.ws.partials + blockIdx.x;
+      Partial* pt = a.ws.partials + g.bid;
       pt->s[0] += v[0];
       pt->s[1] += v[1];
     }
   }
   // 4. sums, decision, tile offsets
   pdl_trigger();
-  finish_by_last_block(a, kind, mode, j, trace, sRed);
+  finish_by_last_block(a, kind, mode, j, trace, sRed, g);
+}
+
+// nblk_hist: CTAs of the evaluation pass (per-CTA child counts in partials c[0]).
+template <bool P2>
+__global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_constant__ OpArgs a, int ns, int kind,
+                                                              int nblk_hist, int mode, int j, int trace) {
+  pdl_wait();
+  select_body<P2>(a, whole_grid(), ns, kind, nblk_hist, mode, j, trace);
 }
 
 // ---------------------------------------------------------------------------
@@ -1662,8 +1692,8 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
 // tile's base (the selection's scan of the tile counts) on, eight consecutive
 // slots per thread and round.  The last CTA to finish writes the output
 // descriptor.  A rejected rotation candidate is not written.
-__global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs a, int ns, int kind) {
-  pdl_wait();
+template <bool C64>
+__device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int kind) {
   __shared__ SelState S;
   __shared__ int sCnt[8][kThreads / 32];  // survivors per (round u, warp)
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -1672,7 +1702,7 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs 
   const long long n = a.in->nnz;
   const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
   const bool ok = ntiles <= a.ws.max_tiles && (long long)ns * n <= a.ws.max_n;
-  if (!ok && blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+  if (!ok && g.bid == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
   const unsigned long long T = S.do_trunc ? S.t_bits : 0ULL;
   const bool incl = !S.do_trunc || S.t_key == ~0ULL;
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
@@ -1680,11 +1710,11 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs 
   double2* oamps = reinterpret_cast<double2*>(a.out->amps);
   float2* oampf = reinterpret_cast<float2*>(a.out->amps);
   const float2* stf = reinterpret_cast<const float2*>(a.ws.tmp_amps);
-  const bool c64 = a.in->amp_type == BASS_AMP_C64;
+  constexpr bool c64 = C64;
   const long long cap = a.out->cap;
   const unsigned lt = (1u << lane) - 1;
   long long written = 0;
-  for (long long b = blockIdx.x; ok && !S.skip_write && b < ntiles; b += gridDim.x) {
+  for (long long b = g.bid; ok && !S.skip_write && b < ntiles; b += g.nblk) {
     long long z0, z1;
     if (kind == K_IDENT) {
       z0 = b * kTile;
@@ -1773,7 +1803,13 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs 
               (unsigned long long)written);
   // the last CTA to finish writes the output descriptor
   pdl_trigger();
-  write_done(a, kind);
+  write_done(a, kind, g);
+}
+
+template <bool C64>
+__global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs a, int ns, int kind) {
+  pdl_wait();
+  compact_body<C64>(a, whole_grid(), ns, kind);
 }
 
 // Rotation step, after the write pass: keep the candidate if accepted.
@@ -1823,24 +1859,44 @@ __global__ void k_rdm_final(const bass_state* st, double* rho, WsView ws, int fi
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <int KIND, int PASS>
-static cudaError_t launch_tile(OpArgs a, int counter, cudaStream_t s, int* grid_out) {
+// Dynamic shared memory of a tile pass and its persistent grid (every CTA
+// that fits at once, at most 1024), set up on first use.
+template <int KIND, int PASS, bool C64>
+static cudaError_t tile_grid(size_t* smem_out, int* grid_out) {
   const size_t smem = (size_t)kTilePad * (16 + 8 + 2 + (PASS == P_WRITE ? 3 : 0));
   static int grid = 0;
   if (grid == 0) {
-    cudaError_t e = cudaFuncSetAttribute(k_tile<KIND, PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_tile<KIND, PASS, C64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<KIND, PASS>, kThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<KIND, PASS, C64>, kThreads, smem);
     if (e != cudaSuccess) return e;
     grid = device().sms * (occ > 0 ? occ : 1);
     if (grid > 1024) grid = 1024;
   }
+  *smem_out = smem;
+  *grid_out = grid;
+  return cudaSuccess;
+}
+
+template <int KIND, int PASS, bool C64>
+static cudaError_t launch_tile_t(OpArgs a, int counter, cudaStream_t s, int* grid_out) {
+  size_t smem = 0;
+  int grid = 0;
+  cudaError_t e = tile_grid<KIND, PASS, C64>(&smem, &grid);
+  if (e != cudaSuccess) return e;
   a.counter = counter;
   a.prof = prof_on() ? 1 : 0;
-  KLAUNCH(KIND * 5 + PASS, s, launch_pdl(k_tile<KIND, PASS>, dim3(grid), dim3(kThreads), smem, s, a));
+  KLAUNCH(KIND * 5 + PASS, s, launch_pdl(k_tile<KIND, PASS, C64>, dim3(grid), dim3(kThreads), smem, s, a));
   if (grid_out) *grid_out = grid;
   return cudaGetLastError();
+}
+
+// the tile pass for the op's amplitude type (a.c64, from the host's record of the state)
+template <int KIND, int PASS>
+static cudaError_t launch_tile(OpArgs a, int counter, cudaStream_t s, int* grid_out) {
+  return a.c64 ? launch_tile_t<KIND, PASS, true>(a, counter, s, grid_out)
+               : launch_tile_t<KIND, PASS, false>(a, counter, s, grid_out);
 }
 
 cudaError_t zero_small(const WsView& ws, cudaStream_t s) {
@@ -1938,9 +1994,14 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
     return launch_tile<KIND, P_WRITE>(a, 3, s, nullptr);
   } else {
     a.prof = prof_on() ? 1 : 0;
-    KLAUNCH(KIND * 5 + P_WRITE, s,
-            launch_pdl(k_compact, dim3(device().sms * 4), dim3(kThreads), 0, s, a, (int)slots_per_entry(KIND),
-                       (int)KIND));
+    if (a.c64)
+      KLAUNCH(KIND * 5 + P_WRITE, s,
+              launch_pdl(k_compact<true>, dim3(device().sms * 4), dim3(kThreads), 0, s, a,
+                         (int)slots_per_entry(KIND), (int)KIND));
+    else
+      KLAUNCH(KIND * 5 + P_WRITE, s,
+              launch_pdl(k_compact<false>, dim3(device().sms * 4), dim3(kThreads), 0, s, a,
+                         (int)slots_per_entry(KIND), (int)KIND));
     return cudaGetLastError();
   }
 }
@@ -1971,9 +2032,10 @@ cudaError_t run_ident_write(OpArgs a, cudaStream_t s) {
 }
 
 cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
-                    cudaStream_t s) {
+                    cudaStream_t s, int c64) {
   cudaError_t e = cudaSuccess;
   OpArgs a{};
+  a.c64 = c64;
   a.in = st;
   a.out = nullptr;
   a.ctrl = ctrl;
@@ -1993,15 +2055,16 @@ cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, 
 // entries by every other bit with q1 at bit 1.  rho: 16 doubles, see k_tile's
 // P_RDM pass for K_GATE2 (set s writes rho[4 s .. 4 s + 3]).
 cudaError_t run_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, double* rho, bass_ctrl* ctrl,
-                       const WsView& ws, cudaStream_t s) {
+                       const WsView& ws, cudaStream_t s, int c64) {
   OpArgs a{};
+  a.c64 = c64;
   a.in = st; a.out = tmp; a.ctrl = ctrl; a.ws = ws; a.q = q2; a.gb = 0;
   bass_trunc none{};
   none.k_cond = -1;
   cudaError_t e = run_merge_op(K_PERM, a, none, 0, 0, s);
   if (e != cudaSuccess) return e;
   OpArgs b{};
-  b.in = tmp; b.out = nullptr; b.ctrl = ctrl; b.ws = ws; b.q = q1; b.gb = 1; b.nsets = 4;
+  b.in = tmp; b.out = nullptr; b.ctrl = ctrl; b.ws = ws; b.q = q1; b.gb = 1; b.nsets = 4; b.c64 = c64;
   // the partition also clears the small workspace region
   KLAUNCH(S_PARTITION, s, launch_pdl(k_partition, dim3(device().grid_small, 1), dim3(256), 0, s, b, (int)K_GATE2, 1));
   if ((e = launch_tile<K_GATE2, P_RDM>(b, 0, s, nullptr)) != cudaSuccess) return e;
@@ -2040,8 +2103,9 @@ __global__ void k_rdm_final_bounded(const bass_state* st, double* rho, WsView ws
 }
 
 cudaError_t run_rdm_prepared(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, const WsView& ws,
-                             cudaStream_t s) {
+                             cudaStream_t s, int c64) {
   OpArgs a{};
+  a.c64 = c64;
   a.in = st;
   a.out = nullptr;
   a.ctrl = ctrl;

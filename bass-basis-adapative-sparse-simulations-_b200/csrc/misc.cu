@@ -12,12 +12,13 @@ enum RedMode { R_NORM2 = 0, R_P2 = 1 };
 // ---------------------------------------------------------------------------
 // reductions over a state (exact): per-CTA partials in ws.red
 // ---------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, bool C64>
 __global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsView ws) {
   __shared__ i128 sRed[8];
   const long long n = st->nnz;
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  const int c64 = st->amp_type == BASS_AMP_C64;
+  constexpr int c64 = C64;
+  const double* amps = st->amps;
   i128 v[1] = {0};
   // eight entries per thread and round, summed exactly in the split
   // accumulators (fx_acc96) and joined once per round
@@ -27,7 +28,7 @@ __global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsVi
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const long long i = i0 + u * stride;
-      x[u] = i < n ? amp_raw(st->amps, i, c64) : make_double2(0.0, 0.0);
+      x[u] = i < n ? amp_raw(amps, i, c64) : make_double2(0.0, 0.0);
     }
     double h = 0.0, l = 0.0;
 #pragma unroll
@@ -155,20 +156,22 @@ __global__ void k_fp_out(WsView ws, uint64_t* out6, bass_ctrl* c, int append, in
 // diagonal gates
 // ---------------------------------------------------------------------------
 // sparse_state.py:178-190: a *= diag[(b_q1 << 1) | b_q2], in place
+template <bool C64>
 __global__ void k_phase2q(bass_state* st, double2 d0, double2 d1, double2 d2, double2 d3, int q1, int q2,
                           bass_ctrl* c) {
   const long long n = st->nnz;
   const int t1 = st->pos[q1], t2 = st->pos[q2];
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  const int c64 = st->amp_type == BASS_AMP_C64;
+  constexpr int c64 = C64;
+  double* amps = st->amps;
   const uint64_t* keys = st->keys;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const uint64_t y = keys[i];
     const int idx = (int)((((y >> t1) & 1ULL) << 1) | ((y >> t2) & 1ULL));
     const double2 d = idx == 0 ? d0 : idx == 1 ? d1 : idx == 2 ? d2 : d3;
-    const double2 v = amp_get(st->amps, i, c64, r0, r1);
-    amp_put(st->amps, i, c64 ? cmul_c64(v, d) : cmul(v, d), c64);
+    const double2 v = amp_get(amps, i, c64, r0, r1);
+    amp_put(amps, i, c64 ? cmul_c64(v, d) : cmul(v, d), c64);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -188,19 +191,21 @@ __global__ void k_phase2q(bass_state* st, double2 d0, double2 d1, double2 d2, do
 
 // 1-qubit diagonal gate: a = g_bb * a; children that are exactly zero are
 // dropped by the reference's kernel, so a zero result raises the compaction flag
+template <bool C64>
 __global__ void k_phase1q(bass_state* st, double2 g0, double2 g1, int q, bass_ctrl* c, WsView ws) {
   const long long n = st->nnz;
   const int t = st->pos[q];
   const double r0 = st->rscale[0], r1 = st->rscale[1];
-  const int c64 = st->amp_type == BASS_AMP_C64;
+  constexpr int c64 = C64;
+  double* amps = st->amps;
   const uint64_t* keys = st->keys;
   bool zero = false;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const double2 g = ((keys[i] >> t) & 1ULL) ? g1 : g0;
-    const double2 a = amp_get(st->amps, i, c64, r0, r1);
+    const double2 a = amp_get(amps, i, c64, r0, r1);
     const double2 v = c64 ? cmul_c64(g, a) : cmul(g, a);
-    amp_put(st->amps, i, v, c64);
+    amp_put(amps, i, v, c64);
     zero |= !cnz(v);
   }
   if (__any_sync(0xffffffffu, zero) && (threadIdx.x & 31) == 0) ws.sel->pad = 1;
@@ -769,8 +774,14 @@ cudaError_t run_dot(const double* u, const double* v, long long n, const bass_st
 cudaError_t run_reduce(const bass_state* st, int mode, double* dest, bass_ctrl* ctrl,
                        const WsView& ws, cudaStream_t s) {
   const int grid = device().grid_small > 1024 ? 1024 : device().grid_small;
-  if (mode == R_NORM2) KLAUNCH(S_REDUCE, s, k_reduce_state<R_NORM2><<<grid, 256, 0, s>>>(st, ws));
-  else KLAUNCH(S_REDUCE, s, k_reduce_state<R_P2><<<grid, 256, 0, s>>>(st, ws));
+  const bool c64 = state_c64(st);
+  if (mode == R_NORM2) {
+    if (c64) KLAUNCH(S_REDUCE, s, k_reduce_state<R_NORM2, true><<<grid, 256, 0, s>>>(st, ws));
+    else KLAUNCH(S_REDUCE, s, k_reduce_state<R_NORM2, false><<<grid, 256, 0, s>>>(st, ws));
+  } else {
+    if (c64) KLAUNCH(S_REDUCE, s, k_reduce_state<R_P2, true><<<grid, 256, 0, s>>>(st, ws));
+    else KLAUNCH(S_REDUCE, s, k_reduce_state<R_P2, false><<<grid, 256, 0, s>>>(st, ws));
+  }
   if (dest) KLAUNCH(S_REDUCE, s, k_red_store<<<1, 256, 0, s>>>(ws, grid, dest));
   else KLAUNCH(S_REDUCE, s, k_pr_final<<<1, 256, 0, s>>>(st, ws, grid, ctrl));
   return cudaGetLastError();
@@ -787,24 +798,33 @@ cudaError_t run_fingerprint(const bass_state* st, double pmin, uint64_t* out6, c
 
 cudaError_t run_renorm(bass_state* st, bass_ctrl* ctrl, const WsView& ws, cudaStream_t s) {
   const int grid = device().grid_small > 1024 ? 1024 : device().grid_small;
-  KLAUNCH(S_REDUCE, s, k_reduce_state<R_NORM2><<<grid, 256, 0, s>>>(st, ws));
+  if (state_c64(st)) KLAUNCH(S_REDUCE, s, k_reduce_state<R_NORM2, true><<<grid, 256, 0, s>>>(st, ws));
+  else KLAUNCH(S_REDUCE, s, k_reduce_state<R_NORM2, false><<<grid, 256, 0, s>>>(st, ws));
   KLAUNCH(S_REDUCE, s, k_renorm_apply<<<1, 256, 0, s>>>(st, ws, grid));
   KLAUNCH(S_SMALL, s, k_materialize<<<device().sms * 4, 256, 0, s>>>(st, ws, ctrl));
   return cudaGetLastError();
 }
 
 cudaError_t run_phase2q(bass_state* st, const double* d, int q1, int q2, bass_ctrl* ctrl, cudaStream_t s) {
-  KLAUNCH(S_PHASE2Q, s, k_phase2q<<<device().sms * 4, 256, 0, s>>>(st, make_double2(d[0], d[1]), make_double2(d[2], d[3]),
-                                             make_double2(d[4], d[5]), make_double2(d[6], d[7]), q1, q2, ctrl));
+  const double2 d0 = make_double2(d[0], d[1]), d1 = make_double2(d[2], d[3]);
+  const double2 d2 = make_double2(d[4], d[5]), d3 = make_double2(d[6], d[7]);
+  if (state_c64(st))
+    KLAUNCH(S_PHASE2Q, s, k_phase2q<true><<<device().sms * 4, 256, 0, s>>>(st, d0, d1, d2, d3, q1, q2, ctrl));
+  else
+    KLAUNCH(S_PHASE2Q, s, k_phase2q<false><<<device().sms * 4, 256, 0, s>>>(st, d0, d1, d2, d3, q1, q2, ctrl));
   return cudaGetLastError();
 }
 
 cudaError_t run_phase1q(bass_state* st, bass_state* tmp, const double* g, int q, bass_ctrl* ctrl,
-                        const WsView& ws, cudaStream_t s) {
+                        const WsView& ws, cudaStream_t s, int c64) {
   cudaError_t e = zero_small(ws, s);
   if (e != cudaSuccess) return e;
-  KLAUNCH(S_PHASE1Q, s, k_phase1q<<<device().sms * 4, 256, 0, s>>>(st, make_double2(g[0], g[1]), make_double2(g[2], g[3]), q,
-                                             ctrl, ws));
+  if (c64)
+    KLAUNCH(S_PHASE1Q, s, k_phase1q<true><<<device().sms * 4, 256, 0, s>>>(st, make_double2(g[0], g[1]),
+                                                                           make_double2(g[2], g[3]), q, ctrl, ws));
+  else
+    KLAUNCH(S_PHASE1Q, s, k_phase1q<false><<<device().sms * 4, 256, 0, s>>>(st, make_double2(g[0], g[1]),
+                                                                            make_double2(g[2], g[3]), q, ctrl, ws));
   OpArgs a{};
   a.in = st;
   a.out = tmp;
@@ -814,6 +834,7 @@ cudaError_t run_phase1q(bass_state* st, bass_state* tmp, const double* g, int q,
   a.guard = 1;
   a.nsets = 1;
   a.k_cond = -1;
+  a.c64 = c64;
   e = run_ident_write(a, s);
   if (e != cudaSuccess) return e;
   KLAUNCH(S_PHASE1Q, s, k_phase1q_fin<<<1, 1, 0, s>>>(st, tmp, ws));

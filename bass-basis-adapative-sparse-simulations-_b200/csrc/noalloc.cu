@@ -86,5 +86,5 @@ extern "C" int bass_rdm_1q_noalloc(const bass_state* st, int64_t max_entries, in
   v.partials = sc->partials;
   v.max_n = kNoAllocMaxEntries;
   v.max_tiles = kNoAllocTiles;
-  return run_rdm_prepared(st, num_qubits, rho, ctrl, v, s) == cudaSuccess ? BASS_OK : BASS_ERR_CUDA;
+  return run_rdm_prepared(st, num_qubits, rho, ctrl, v, s, state_c64(st)) == cudaSuccess ? BASS_OK : BASS_ERR_CUDA;
 }

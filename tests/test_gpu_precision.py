@@ -89,9 +89,10 @@ def test_c64_gates_track_c128(env):
         st._topk(nat.trunc(30000, 30000, 3, 2))
     assert s128.nnz == 30000
     assert np.array_equal(s64.x, s128.x)
-    assert abs(s64.gamma - s128.gamma) <= 1e-12
+    assert abs(s64.gamma - s128.gamma) <= 1e-6 * s128.gamma   # kept mass of float-rounded inputs
     f = abs(np.vdot(s128.alpha, s64.alpha.astype(np.complex128))) ** 2
-    assert f >= 1 - 1e-10
+    # rounding the renormalised amplitudes to float moves the norm by ~1e-10
+    assert f >= 1 - 1e-8
 
 
 def test_c64_norm_pr_rdm_are_fp64(env):
