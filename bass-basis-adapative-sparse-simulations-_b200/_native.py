@@ -70,6 +70,13 @@ class Trunc(ctypes.Structure):
 
 NO_TRUNC = Trunc(-1, 0, 0, 0, 0, 0)
 
+# bass_seg_op (include/bass_b200.h), one segment of a batched op
+SEG_OP_DTYPE = np.dtype([("in", "<u8"), ("tmp", "<u8"), ("out", "<u8"), ("ctrl", "<u8"), ("ws", "<u8"),
+                         ("ws_bytes", "<u8"), ("G", "<f8", (32,)), ("q1", "<i4"), ("q2", "<i4"),
+                         ("k_cond", "<i8"), ("k_keep", "<i8"), ("gamma_mode", "<i4"), ("renorm", "<i4"),
+                         ("mark_active", "<i4"), ("trace", "<i4"), ("rho", "<u8"), ("num_qubits", "<i4"),
+                         ("pad", "<i4")], align=True)
+
 
 class BassError(RuntimeError):
     pass
@@ -129,6 +136,14 @@ def load_library():
         "bass_radix_sort_u64": (I32, [P, P, I64, I32, P, SZ, P, P]),
         "bass_merge_sorted": (I32, [P, P, I64, P, P, SZ, P, P]),
         "bass_error": (I32, [P, P]),
+        "bass_batch_ws_bytes": (SZ, [I32]),
+        "bass_gate_1q_batch": (I32, [P, I32, P, SZ, P]),
+        "bass_gate_2q_batch": (I32, [P, I32, P, SZ, P]),
+        "bass_phase_2q_batch": (I32, [P, I32, P, SZ, P]),
+        "bass_topk_batch": (I32, [P, I32, P, SZ, P]),
+        "bass_rotate_step_batch": (I32, [P, I32, P, SZ, P]),
+        "bass_rdm_1q_batch": (I32, [P, I32, P, SZ, P]),
+        "bass_pr_batch": (I32, [P, I32, I32, P, SZ, P]),
         "bass_launch_count": (I64, []),
         "bass_profile_enable": (None, [I32]),
         "bass_profile_collect": (I32, [P, P, I32]),
@@ -168,7 +183,7 @@ class Engine:
     """Per-stream device context: control block, workspace, optional trace."""
 
     def __init__(self, max_n: int, num_qubits: int, trace_cap: int = 0, pr_tie_tol: float = 1e-12,
-                 device=None):
+                 device=None, ctrl=None, rho=None):
         import torch
         self.L = lib()
         self.torch = torch
@@ -177,11 +192,14 @@ class Engine:
         self.nq = int(num_qubits)
         self.ws_bytes = int(self.L.bass_workspace_bytes(self.max_n // 4, self.max_n, self.nq))
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
-        self.ctrl = torch.zeros(self.L.bass_ctrl_bytes(), dtype=torch.uint8, device=self.device)
+        # ctrl / rho: optional views into larger device tensors (a batch keeps
+        # every state's control block and moments contiguous, to read them at once)
+        self.ctrl = ctrl if ctrl is not None else torch.zeros(self.L.bass_ctrl_bytes(), dtype=torch.uint8,
+                                                               device=self.device)
         self.trace_cap = int(trace_cap)
         self.trace = (torch.zeros(max(trace_cap, 1) * TRACE_WORDS, dtype=torch.int64, device=self.device)
                       if trace_cap else None)
-        self.rho = torch.zeros(4 * 64, dtype=torch.float64, device=self.device)
+        self.rho = rho if rho is not None else torch.zeros(4 * 64, dtype=torch.float64, device=self.device)
         self.scratch_f64 = torch.zeros(8, dtype=torch.float64, device=self.device)
         self.scratch_u64 = torch.zeros(8, dtype=torch.int64, device=self.device)
         self.pr_tie_tol = float(pr_tie_tol)

@@ -68,3 +68,44 @@ def config1_circuit(seed=0, num_qubits=24, num_layers=20):
 def config2_circuit(seed=0, num_qubits=40, depth=30):
     """Brickwork workload: Haar SU(2) layers, CZ pairs skipped with p=1/2."""
     return brickwork_circuit(num_qubits, depth, rng=np.random.default_rng(seed))
+
+
+def config4_batch(seed=0, count=256, n_range=(16, 48), layer_range=(10, 60), h_range=(0.3, 2.0),
+                  m_range=(10, 20), dt=0.05, disorder_h=0.0):
+    """The batched workload: ``count`` TFIM Trotter circuits (J = 1) with the
+    qubit count, layer count, field h (one per circuit) and budget K = 2^m
+    drawn uniformly per circuit from one seeded generator.  Returns
+    (specs, circuits) with specs[i] = (n, K).  ``disorder_h`` > 0 draws every
+    site's field from [h - disorder_h, h + disorder_h] instead (a uniform
+    field makes many |a|^2 exactly equal, so top-k ties are common)."""
+    rng = np.random.default_rng(seed)
+    specs, circuits = [], []
+    for _ in range(count):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        layers = int(rng.integers(layer_range[0], layer_range[1] + 1))
+        h = float(rng.uniform(h_range[0], h_range[1]))
+        m = int(rng.integers(m_range[0], m_range[1] + 1))
+        circuits.append(tfim_circuit(n, layers, J=1.0, h=h, dt=dt, rng=rng, disorder_strength_h=disorder_h))
+        specs.append((n, 2 ** m))
+    return specs, circuits
+
+
+def config5_requests(seed=0, count=100, tfim=None, brick_n=(20, 44), brick_depth=(10, 30), brick_m=(12, 22)):
+    """The served workload: ``count`` requests (circuit, n, K), each drawn with
+    probability 1/2 from the batched workload's TFIM distribution
+    (``config4_batch`` arguments in ``tfim``) or as a brickwork circuit with n,
+    depth and K = 2^m uniform in the given ranges; one seeded generator."""
+    rng = np.random.default_rng(seed)
+    tfim = dict(tfim or {})
+    out = []
+    for _ in range(count):
+        if rng.random() < 0.5:
+            sub = int(rng.integers(0, 2 ** 31))
+            (spec,), (circ,) = config4_batch(seed=sub, count=1, **tfim)
+            out.append((circ, spec[0], spec[1]))
+        else:
+            n = int(rng.integers(brick_n[0], brick_n[1] + 1))
+            depth = int(rng.integers(brick_depth[0], brick_depth[1] + 1))
+            m = int(rng.integers(brick_m[0], brick_m[1] + 1))
+            out.append((brickwork_circuit(n, depth, rng=rng), n, 2 ** m))
+    return out

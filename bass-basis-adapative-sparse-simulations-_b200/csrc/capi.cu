@@ -512,3 +512,195 @@ int bass_error(bass_ctrl* ctrl, void* stream) {
 }
 
 }  // extern "C"
+
+// ---- batched (segmented) ops ---------------------------------------------------
+namespace bass {
+static size_t batch_ops_bytes(int max_ops) { return align256((size_t)max_ops * sizeof(OpArgs)); }
+
+struct BatchView {
+  SegPlan* plan;
+  OpArgs* ops_a;
+  OpArgs* ops_b;
+};
+
+static bool carve_batch(void* ws, size_t bytes, int n, BatchView* v) {
+  if (!ws || ((uintptr_t)ws & 255) || n < 1 || n > kMaxSeg) return false;
+  const size_t need = align256(sizeof(SegPlan)) + 2 * batch_ops_bytes(n);
+  if (bytes < need) return false;
+  char* b = static_cast<char*>(ws);
+  v->plan = reinterpret_cast<SegPlan*>(b);
+  v->ops_a = reinterpret_cast<OpArgs*>(b + align256(sizeof(SegPlan)));
+  v->ops_b = reinterpret_cast<OpArgs*>(b + align256(sizeof(SegPlan)) + batch_ops_bytes(n));
+  return true;
+}
+
+// The single-state op of one segment (the fields every kind shares); returns
+// false if the segment's arguments are invalid.
+static bool seg_common(const bass_seg_op& o, OpArgs* a) {
+  *a = OpArgs{};
+  if (!o.in || !o.ctrl || !carve(o.ws, o.ws_bytes, &a->ws)) return false;
+  a->in = o.in;
+  a->out = o.out;
+  a->ctrl = o.ctrl;
+  a->nsets = 1;
+  a->fin = 1;
+  a->k_cond = o.tr.k_cond;
+  a->k_keep = o.tr.k_keep;
+  a->tr = o.tr;
+  a->tr.trace = 0;
+  a->prof = prof_on() ? 1 : 0;
+  a->c64 = state_c64(o.in);
+  return true;
+}
+
+// Copies n ops to the device (the host array is pageable, so the copy is
+// staged before this returns and the array may be reused at once).
+static cudaError_t upload(OpArgs* dev, const std::vector<OpArgs>& host, cudaStream_t s) {
+  return cudaMemcpyAsync(dev, host.data(), host.size() * sizeof(OpArgs), cudaMemcpyHostToDevice, s);
+}
+
+static int same_type(const std::vector<OpArgs>& v) {
+  for (const OpArgs& a : v)
+    if (a.c64 != v[0].c64) return 0;
+  return 1;
+}
+}  // namespace bass
+
+extern "C" {
+
+size_t bass_batch_ws_bytes(int max_ops) {
+  if (max_ops < 1) max_ops = 1;
+  return align256(sizeof(SegPlan)) + 2 * batch_ops_bytes(max_ops);
+}
+
+#define BATCH_PROLOGUE()                                          \
+  if (!ops || n < 1 || n > kMaxSeg) return BASS_ERR_ARG;          \
+  BatchView bv;                                                   \
+  if (!carve_batch(batch_ws, batch_ws_bytes, n, &bv)) return BASS_ERR_WORKSPACE; \
+  cudaStream_t s = (cudaStream_t)stream;                          \
+  std::vector<OpArgs> A((size_t)n);
+
+int bass_gate_1q_batch(const bass_seg_op* ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream) {
+  BATCH_PROLOGUE();
+  for (int i = 0; i < n; ++i) {
+    const bass_seg_op& o = ops[i];
+    if (!seg_common(o, &A[i]) || !o.out || o.out == o.in || o.q1 < 0 || o.q1 >= BASS_MAX_QUBITS) return BASS_ERR_ARG;
+    A[i].q = o.q1;
+    load_G(A[i], o.G, 4);
+  }
+  if (!same_type(A)) return BASS_ERR_ARG;
+  cudaError_t e = upload(bv.ops_a, A, s);
+  if (e == cudaSuccess) e = run_merge_op_seg(K_GATE1, bv.ops_a, n, A[0].c64, 0, 0, bv.plan, s);
+  return status_of(e);
+}
+
+int bass_gate_2q_batch(const bass_seg_op* ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream) {
+  BATCH_PROLOGUE();
+  std::vector<OpArgs> B((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    const bass_seg_op& o = ops[i];
+    if (!seg_common(o, &A[i]) || !o.tmp || !o.out || o.in == o.tmp || o.tmp == o.out || o.in == o.out ||
+        o.q1 < 0 || o.q2 < 0 || o.q1 >= BASS_MAX_QUBITS || o.q2 >= BASS_MAX_QUBITS || o.q1 == o.q2)
+      return BASS_ERR_ARG;
+    B[i] = A[i];
+    // pass 1: q2 to the lowest physical bit (a reorder, into tmp)
+    A[i].out = o.tmp;
+    A[i].q = o.q2;
+    A[i].write_mode = 2;
+    A[i].counter = 3;
+    A[i].k_cond = -1;
+    A[i].tr = bass_trunc{};
+    A[i].tr.k_cond = -1;
+    // pass 2: groups of four on q1 above it, from tmp
+    B[i].in = o.tmp;
+    B[i].q = o.q1;
+    B[i].gb = 1;
+    load_G(B[i], o.G, 16);
+  }
+  if (!same_type(A)) return BASS_ERR_ARG;
+  cudaError_t e = upload(bv.ops_a, A, s);
+  if (e == cudaSuccess) e = upload(bv.ops_b, B, s);
+  if (e == cudaSuccess) e = run_merge_op_seg(K_PERM, bv.ops_a, n, A[0].c64, 0, 0, bv.plan, s);
+  if (e == cudaSuccess) e = run_merge_op_seg(K_GATE2, bv.ops_b, n, A[0].c64, 0, 0, bv.plan, s);
+  return status_of(e);
+}
+
+int bass_phase_2q_batch(const bass_seg_op* ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream) {
+  BATCH_PROLOGUE();
+  for (int i = 0; i < n; ++i) {
+    const bass_seg_op& o = ops[i];
+    if (!seg_common(o, &A[i]) || o.q1 < 0 || o.q2 < 0 || o.q1 >= BASS_MAX_QUBITS || o.q2 >= BASS_MAX_QUBITS ||
+        o.q1 == o.q2)
+      return BASS_ERR_ARG;
+    A[i].q = o.q1;
+    A[i].j = o.q2;
+    load_G(A[i], o.G, 4);
+  }
+  if (!same_type(A)) return BASS_ERR_ARG;
+  cudaError_t e = upload(bv.ops_a, A, s);
+  if (e == cudaSuccess) e = run_phase2q_seg(bv.ops_a, n, A[0].c64, s);
+  return status_of(e);
+}
+
+int bass_topk_batch(const bass_seg_op* ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream) {
+  BATCH_PROLOGUE();
+  for (int i = 0; i < n; ++i) {
+    const bass_seg_op& o = ops[i];
+    if (!seg_common(o, &A[i]) || !o.out || o.out == o.in) return BASS_ERR_ARG;
+  }
+  if (!same_type(A)) return BASS_ERR_ARG;
+  cudaError_t e = upload(bv.ops_a, A, s);
+  if (e == cudaSuccess) e = run_merge_op_seg(K_IDENT, bv.ops_a, n, A[0].c64, 0, 0, bv.plan, s);
+  return status_of(e);
+}
+
+int bass_rotate_step_batch(const bass_seg_op* ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream) {
+  BATCH_PROLOGUE();
+  for (int i = 0; i < n; ++i) {
+    const bass_seg_op& o = ops[i];
+    if (!seg_common(o, &A[i]) || !o.tmp || o.tmp == o.in || o.q1 < 0 || o.q1 >= 64 || o.tr.k_keep < 0)
+      return BASS_ERR_ARG;
+    A[i].out = o.tmp;
+    A[i].q = o.q1;
+    A[i].j = o.q1;
+    A[i].k_cond = o.tr.k_keep;
+    A[i].k_keep = o.tr.k_keep;
+    A[i].fin_mode = 1;
+    A[i].commit = 1;
+    load_G(A[i], o.G, 4);
+  }
+  if (!same_type(A)) return BASS_ERR_ARG;
+  cudaError_t e = upload(bv.ops_a, A, s);
+  if (e == cudaSuccess) e = run_merge_op_seg(K_ROT1, bv.ops_a, n, A[0].c64, 1, 0, bv.plan, s);
+  return status_of(e);
+}
+
+int bass_rdm_1q_batch(const bass_seg_op* ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream) {
+  BATCH_PROLOGUE();
+  int max_nq = 1;
+  for (int i = 0; i < n; ++i) {
+    const bass_seg_op& o = ops[i];
+    if (!seg_common(o, &A[i]) || !o.rho || o.num_qubits < 1 || o.num_qubits > BASS_MAX_QUBITS) return BASS_ERR_ARG;
+    A[i].nsets = o.num_qubits;
+    A[i].rho = o.rho;
+    A[i].fin = 0;
+    if (o.num_qubits > max_nq) max_nq = o.num_qubits;
+  }
+  if (!same_type(A)) return BASS_ERR_ARG;
+  cudaError_t e = upload(bv.ops_a, A, s);
+  if (e == cudaSuccess) e = run_rdm_seg(bv.ops_a, n, max_nq, A[0].c64, bv.plan, s);
+  return status_of(e);
+}
+
+int bass_pr_batch(const bass_seg_op* ops, int n, int mode, void* batch_ws, size_t batch_ws_bytes, void* stream) {
+  BATCH_PROLOGUE();
+  if (mode != 0 && mode != 1) return BASS_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (!seg_common(ops[i], &A[i])) return BASS_ERR_ARG;
+  if (!same_type(A)) return BASS_ERR_ARG;
+  cudaError_t e = upload(bv.ops_a, A, s);
+  if (e == cudaSuccess) e = run_reduce_seg(bv.ops_a, n, mode, A[0].c64, s);
+  return status_of(e);
+}
+
+}  // extern "C"

@@ -38,6 +38,16 @@ struct OpArgs {
   double* rho;    // RDM moments of a segmented RDM (4 per qubit)
 };
 
+// Segmented launches: one op on each of up to kMaxSeg states in one launch.
+// The grid is split into one block group per state, sized by the state's
+// share of the op's work (every state gets at least one block).
+constexpr int kMaxSeg = 1024;
+struct SegPlan {
+  int nseg;
+  int kind;
+  long long wp[kMaxSeg + 1];  // exclusive prefix of the states' work weights
+};
+
 enum Slot {
   S_PARTITION = 30, S_SELECT1 = 31, S_SELECT2 = 32, S_SELECT_EXACT = 33, S_FINALIZE = 34, S_REDUCE = 35,
   S_FINGERPRINT = 36, S_PHASE2Q = 37, S_PHASE1Q = 38, S_RDM_FINAL = 39, S_SORT = 40, S_MERGE_RUNS = 41,
@@ -114,6 +124,15 @@ cudaError_t run_ident_write(OpArgs a, cudaStream_t s);
 // rotation step: keep the candidate in *tmp if the decision accepted it
 cudaError_t run_commit(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const WsView& ws, int j, int trace,
                        cudaStream_t s);
+
+// merge.cu, segmented: ops_dev holds nseg OpArgs (all of one amplitude type),
+// plan_dev is scratch for the block groups
+cudaError_t run_merge_op_seg(int kind, const OpArgs* ops_dev, int nseg, int c64, int fin_mode, int trace,
+                             SegPlan* plan_dev, cudaStream_t s);
+cudaError_t run_rdm_seg(const OpArgs* ops_dev, int nseg, int max_nq, int c64, SegPlan* plan_dev, cudaStream_t s);
+// misc.cu, segmented: diagonal 2-qubit phases; PR (mode 1) or renormalisation (mode 0)
+cudaError_t run_phase2q_seg(const OpArgs* ops_dev, int nseg, int c64, cudaStream_t s);
+cudaError_t run_reduce_seg(const OpArgs* ops_dev, int nseg, int mode, int c64, cudaStream_t s);
 
 // misc.cu
 struct DenseG4 {

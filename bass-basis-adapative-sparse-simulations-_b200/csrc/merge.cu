@@ -2120,4 +2120,239 @@ cudaError_t run_rdm_prepared(const bass_state* st, int nq, double* rho, bass_ctr
   return cudaGetLastError();
 }
 
+
+// ---------------------------------------------------------------------------
+// segmented launches: one op on each of many states per launch
+// ---------------------------------------------------------------------------
+// Group g of a grid of N blocks over S states starts at
+// start(s) = s + (N - S) * wp[s] / W, W = wp[S]: every state gets at least
+// one block and the rest are shared in proportion to the work weights.
+__device__ __forceinline__ long long seg_start(const SegPlan* plan, int s, long long N) {
+  const int S = plan->nseg;
+  const long long W = plan->wp[S] > 0 ? plan->wp[S] : 1;
+  return (long long)s + ((N - S) * plan->wp[s]) / W;
+}
+
+// Blocks of state s's group in a grid of N blocks.
+__device__ __forceinline__ int seg_size(const SegPlan* plan, int s, long long N) {
+  return (int)(seg_start(plan, s + 1, N) - seg_start(plan, s, N));
+}
+
+// This block's state (the last s with start(s) <= blockIdx.x) and group; the
+// state's op is copied into *sa.  Called by the whole block.
+__device__ Grp seg_enter(const OpArgs* ops, const SegPlan* plan, OpArgs* sa, int* seg_out) {
+  __shared__ int sSeg, sBid, sN;
+  if (threadIdx.x == 0) {
+    const long long N = gridDim.x, b = blockIdx.x;
+    int lo = 0, hi = plan->nseg - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (seg_start(plan, mid, N) <= b) lo = mid;
+      else hi = mid - 1;
+    }
+    sSeg = lo;
+    sBid = (int)(b - seg_start(plan, lo, N));
+    sN = seg_size(plan, lo, N);
+  }
+  __syncthreads();
+  constexpr int kWords = (int)(sizeof(OpArgs) / 8);
+  static_assert(sizeof(OpArgs) % 8 == 0, "op words");
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(ops + sSeg);
+  unsigned long long* dst = reinterpret_cast<unsigned long long*>(sa);
+  for (int i = threadIdx.x; i < kWords; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  if (seg_out) *seg_out = sSeg;
+  return Grp{sBid, sN};
+}
+
+// The block groups of an op: work weight of state s = its input entries plus
+// one tile (times its qubits for an RDM).  One block.
+__global__ void k_seg_plan(const OpArgs* ops, int nseg, int kind, SegPlan* plan) {
+  __shared__ long long sW[kMaxSeg];
+  for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
+    const long long n = ops[s].in->nnz;
+    sW[s] = (n + kStep) * (kind == K_RDM ? (long long)ops[s].nsets : 1LL);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long run = 0;
+    for (int s = 0; s < nseg; ++s) {
+      plan->wp[s] = run;
+      run += sW[s];
+    }
+    plan->wp[nseg] = run;
+    plan->nseg = nseg;
+    plan->kind = kind;
+  }
+}
+
+__global__ void k_partition_seg(const OpArgs* ops, const SegPlan* plan, int kind, int zero) {
+  __shared__ OpArgs sa;
+  const Grp g = seg_enter(ops, plan, &sa, nullptr);
+  if (kind == K_IDENT) {  // no merge: only the op's workspace region is cleared
+    if (zero && blockIdx.y == 0) zero_op_region(sa, g);
+    return;
+  }
+  if (kind == K_RDM && (int)blockIdx.y >= sa.nsets) return;  // qubits this state does not have
+  partition_body(sa, kind, zero, blockIdx.y, g);
+}
+
+template <int KIND, int PASS, bool C64>
+__global__ void __launch_bounds__(kThreads, 4) k_tile_seg(const OpArgs* ops, const SegPlan* plan) {
+  __shared__ OpArgs sa;
+  const Grp g = seg_enter(ops, plan, &sa, nullptr);
+  tile_body<KIND, PASS, C64>(sa, g);
+}
+
+// nblk_hist: grid of the evaluation pass; this state's evaluation group wrote
+// its per-CTA child counts to partials[0 .. its group size).
+template <bool P2>
+__global__ void __launch_bounds__(kSelThreads) k_select_seg(const OpArgs* ops, const SegPlan* plan, int ns, int kind,
+                                                             int nblk_hist, int mode, int trace) {
+  __shared__ OpArgs sa;
+  int seg = 0;
+  const Grp g = seg_enter(ops, plan, &sa, &seg);
+  select_body<P2>(sa, g, ns, kind, seg_size(plan, seg, nblk_hist), mode, sa.j, trace);
+}
+
+template <bool C64>
+__global__ void __launch_bounds__(256) k_compact_seg(const OpArgs* ops, const SegPlan* plan, int ns, int kind) {
+  __shared__ OpArgs sa;
+  const Grp g = seg_enter(ops, plan, &sa, nullptr);
+  compact_body<C64>(sa, g, ns, kind);
+}
+
+// per state, the moments of each of its qubits (grid: qubit x state)
+__global__ void k_rdm_final_seg(const OpArgs* ops) {
+  __shared__ i128 sRed[4 * 8];
+  const OpArgs& a = ops[blockIdx.y];
+  const int set = blockIdx.x;
+  if (set >= a.nsets) return;
+  const long long ntiles = merge_tiles(a.in->nnz);
+  if (ntiles > a.ws.max_tiles) {
+    if (threadIdx.x == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+    return;
+  }
+  i128 v[4] = {0, 0, 0, 0};
+  for (long long t = threadIdx.x; t < ntiles; t += blockDim.x) {
+    const Partial& p = a.ws.partials[(long long)set * a.ws.max_tiles + t];
+    v[0] += p.s[0]; v[1] += p.s[1]; v[2] += p.s[2]; v[3] += p.s[3];
+  }
+  block_sum_i128<4>(v, sRed);
+  if (threadIdx.x == 0) {
+    double* r = a.rho + 4 * set;
+    r[0] = fx_to(v[0]);
+    r[1] = fx_to(v[1]);
+    r[2] = fx_to(v[2]);
+    r[3] = fx_to(v[3]);
+  }
+}
+
+
+// Grid of a segmented kernel: every block of it that fits at once, and at
+// least one block per state.
+template <typename F>
+static int seg_grid(F kern, int threads, size_t smem, int nseg) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem) != cudaSuccess || occ < 1) occ = 1;
+  const int g = device().sms * occ;
+  return g > nseg ? g : nseg;
+}
+
+template <int KIND, bool C64>
+static cudaError_t merge_op_seg(const OpArgs* ops, int nseg, int fin_mode, int trace, SegPlan* plan,
+                                cudaStream_t s) {
+  KLAUNCH(S_SMALL, s, k_seg_plan<<<1, 1024, 0, s>>>(ops, nseg, KIND, plan));
+  const int np = device().grid_small > nseg ? device().grid_small : nseg;
+  KLAUNCH(S_PARTITION, s, k_partition_seg<<<dim3(np, 1), 256, 0, s>>>(ops, plan, KIND, 1));
+  constexpr int PASS = KIND == K_PERM ? P_WRITE : P_HIST;
+  const size_t smem = (size_t)kTilePad * (16 + 8 + 2 + (PASS == P_WRITE ? 3 : 0));
+  static int nt = 0;
+  if (nt == 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_seg<KIND, PASS, C64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    nt = seg_grid(k_tile_seg<KIND, PASS, C64>, kThreads, smem, 1);
+  }
+  const int gt = nt > nseg ? nt : nseg;
+  KLAUNCH(KIND * 5 + PASS, s, k_tile_seg<KIND, PASS, C64><<<gt, kThreads, smem, s>>>(ops, plan));
+  if (KIND == K_PERM) return cudaGetLastError();
+  constexpr int ns = slots_per_entry(KIND);
+  const size_t ssmem = (size_t)kCandSmem * 16;
+  cudaError_t e = cudaSuccess;
+  if (fin_mode == 1) {
+    static int gs1 = 0;
+    if (gs1 == 0) {
+      if ((e = cudaFuncSetAttribute(k_select_seg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem)) !=
+          cudaSuccess)
+        return e;
+      gs1 = seg_grid(k_select_seg<true>, kSelThreads, ssmem, 1);
+      if (gs1 > 1024) gs1 = 1024;
+    }
+    if (nseg > gs1) return cudaErrorInvalidValue;  // the groups' barriers need every block resident
+    KLAUNCH(S_SELECT1, s, e = launch_coop(k_select_seg<true>, dim3(gs1), dim3(kSelThreads), ssmem, s, ops, plan, ns,
+                                          (int)KIND, gt, fin_mode, trace));
+  } else {
+    static int gs0 = 0;
+    if (gs0 == 0) {
+      if ((e = cudaFuncSetAttribute(k_select_seg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem)) !=
+          cudaSuccess)
+        return e;
+      gs0 = seg_grid(k_select_seg<false>, kSelThreads, ssmem, 1);
+      if (gs0 > 1024) gs0 = 1024;
+    }
+    if (nseg > gs0) return cudaErrorInvalidValue;
+    KLAUNCH(S_SELECT1, s, e = launch_coop(k_select_seg<false>, dim3(gs0), dim3(kSelThreads), ssmem, s, ops, plan, ns,
+                                          (int)KIND, gt, fin_mode, trace));
+  }
+  if (e != cudaSuccess) return e;
+  const int gc = device().sms * 4 > nseg ? device().sms * 4 : nseg;
+  KLAUNCH(KIND * 5 + P_WRITE, s, k_compact_seg<C64><<<gc, kThreads, 0, s>>>(ops, plan, ns, (int)KIND));
+  return cudaGetLastError();
+}
+
+template <int KIND>
+static cudaError_t merge_op_seg_t(const OpArgs* ops, int nseg, int c64, int fin_mode, int trace, SegPlan* plan,
+                                  cudaStream_t s) {
+  return c64 ? merge_op_seg<KIND, true>(ops, nseg, fin_mode, trace, plan, s)
+             : merge_op_seg<KIND, false>(ops, nseg, fin_mode, trace, plan, s);
+}
+
+cudaError_t run_merge_op_seg(int kind, const OpArgs* ops, int nseg, int c64, int fin_mode, int trace,
+                             SegPlan* plan, cudaStream_t s) {
+  if (nseg < 1 || nseg > kMaxSeg) return cudaErrorInvalidValue;
+  switch (kind) {
+    case K_GATE1: return merge_op_seg_t<K_GATE1>(ops, nseg, c64, fin_mode, trace, plan, s);
+    case K_ROT1: return merge_op_seg_t<K_ROT1>(ops, nseg, c64, fin_mode, trace, plan, s);
+    case K_GATE2: return merge_op_seg_t<K_GATE2>(ops, nseg, c64, fin_mode, trace, plan, s);
+    case K_PERM: return merge_op_seg_t<K_PERM>(ops, nseg, c64, fin_mode, trace, plan, s);
+    case K_IDENT: return merge_op_seg_t<K_IDENT>(ops, nseg, c64, fin_mode, trace, plan, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <bool C64>
+static cudaError_t rdm_seg(const OpArgs* ops, int nseg, int max_nq, SegPlan* plan, cudaStream_t s) {
+  KLAUNCH(S_SMALL, s, k_seg_plan<<<1, 1024, 0, s>>>(ops, nseg, K_RDM, plan));
+  const int np = device().grid_small > nseg ? device().grid_small : nseg;
+  KLAUNCH(S_PARTITION, s, k_partition_seg<<<dim3(np, max_nq), 256, 0, s>>>(ops, plan, K_RDM, 1));
+  const size_t smem = (size_t)kTilePad * (16 + 8 + 2);
+  static int nt = 0;
+  if (nt == 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_seg<K_RDM, P_RDM, C64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    nt = seg_grid(k_tile_seg<K_RDM, P_RDM, C64>, kThreads, smem, 1);
+  }
+  const int gt = nt > nseg ? nt : nseg;
+  KLAUNCH(K_RDM * 5 + P_RDM, s, k_tile_seg<K_RDM, P_RDM, C64><<<gt, kThreads, smem, s>>>(ops, plan));
+  KLAUNCH(S_RDM_FINAL, s, k_rdm_final_seg<<<dim3(max_nq, nseg), 256, 0, s>>>(ops));
+  return cudaGetLastError();
+}
+
+cudaError_t run_rdm_seg(const OpArgs* ops, int nseg, int max_nq, int c64, SegPlan* plan, cudaStream_t s) {
+  if (nseg < 1 || nseg > kMaxSeg || max_nq < 1 || max_nq > kMaxSets) return cudaErrorInvalidValue;
+  return c64 ? rdm_seg<true>(ops, nseg, max_nq, plan, s) : rdm_seg<false>(ops, nseg, max_nq, plan, s);
+}
+
 }  // namespace bass

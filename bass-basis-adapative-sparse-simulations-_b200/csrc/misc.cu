@@ -13,7 +13,7 @@ enum RedMode { R_NORM2 = 0, R_P2 = 1 };
 // reductions over a state (exact): per-CTA partials in ws.red
 // ---------------------------------------------------------------------------
 template <int MODE, bool C64>
-__global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsView ws) {
+__device__ __forceinline__ void reduce_body(const bass_state* st, const WsView& ws, int bid, int nblk) {
   __shared__ i128 sRed[8];
   const long long n = st->nnz;
   const double r0 = st->rscale[0], r1 = st->rscale[1];
@@ -22,8 +22,8 @@ __global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsVi
   i128 v[1] = {0};
   // eight entries per thread and round, summed exactly in the split
   // accumulators (fx_acc96) and joined once per round
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 8 * stride) {
+  const long long stride = (long long)nblk * blockDim.x;
+  for (long long i0 = (long long)bid * blockDim.x + threadIdx.x; i0 < n; i0 += 8 * stride) {
     double2 x[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -39,7 +39,19 @@ __global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsVi
     v[0] += fx_join96s(h, l);
   }
   block_sum_i128<1>(v, sRed);
-  if (threadIdx.x == 0) ws.red[blockIdx.x] = v[0];
+  if (threadIdx.x == 0) ws.red[bid] = v[0];
+}
+
+template <int MODE, bool C64>
+__global__ void __launch_bounds__(256) k_reduce_state(const bass_state* st, WsView ws) {
+  reduce_body<MODE, C64>(st, ws, blockIdx.x, gridDim.x);
+}
+
+// segmented: state blockIdx.y of the ops, gridDim.x blocks each
+template <int MODE, bool C64>
+__global__ void __launch_bounds__(256) k_reduce_state_seg(const OpArgs* ops) {
+  const OpArgs& a = ops[blockIdx.y];
+  reduce_body<MODE, C64>(a.in, a.ws, blockIdx.x, gridDim.x);
 }
 
 __device__ __forceinline__ double reduce_red(const WsView& ws, int nblk, i128* sRed) {
@@ -57,7 +69,7 @@ __global__ void k_red_store(WsView ws, int nblk, double* dest) {
 }
 
 // bass_simulator.py:574-578 _pr
-__global__ void k_pr_final(const bass_state* st, WsView ws, int nblk, bass_ctrl* c) {
+__device__ __forceinline__ void pr_final_body(const bass_state* st, const WsView& ws, int nblk, bass_ctrl* c) {
   __shared__ i128 sRed[8];
   const double S = reduce_red(ws, nblk, sRed);
   if (threadIdx.x == 0) {
@@ -66,11 +78,16 @@ __global__ void k_pr_final(const bass_state* st, WsView ws, int nblk, bass_ctrl*
     c->pr_cur = pr;
   }
 }
+__global__ void k_pr_final(const bass_state* st, WsView ws, int nblk, bass_ctrl* c) { pr_final_body(st, ws, nblk, c); }
+__global__ void k_pr_final_seg(const OpArgs* ops, int nblk) {
+  const OpArgs& a = ops[blockIdx.x];
+  pr_final_body(a.in, a.ws, nblk, a.ctrl);
+}
 
 // bass_simulator.py:551-554 _renorm: norm = sqrt(sum |a|^2); if norm > 1e-30 the
 // amplitudes become a * (1/norm).  The factor goes to a free rscale slot; if
 // both are taken the array is rewritten first (k_materialize).
-__global__ void k_renorm_apply(bass_state* st, WsView ws, int nblk) {
+__device__ __forceinline__ void renorm_apply_body(bass_state* st, const WsView& ws, int nblk) {
   __shared__ i128 sRed[8];
   const double S = reduce_red(ws, nblk, sRed);
   if (threadIdx.x != 0) return;
@@ -85,25 +102,36 @@ __global__ void k_renorm_apply(bass_state* st, WsView ws, int nblk) {
     ws.sel->kept = r;
   }
 }
+__global__ void k_renorm_apply(bass_state* st, WsView ws, int nblk) { renorm_apply_body(st, ws, nblk); }
+__global__ void k_renorm_apply_seg(const OpArgs* ops, int nblk) {
+  const OpArgs& a = ops[blockIdx.x];
+  renorm_apply_body(const_cast<bass_state*>(a.in), a.ws, nblk);
+}
 
-__global__ void k_materialize(bass_state* st, WsView ws, bass_ctrl* c) {
+__device__ __forceinline__ void materialize_body(bass_state* st, const WsView& ws, bass_ctrl* c, int bid, int nblk) {
   if (ws.sel->pad != 3) return;
   const long long n = st->nnz;
   const double r0 = st->rscale[0], r1 = st->rscale[1];
   const int c64 = st->amp_type == BASS_AMP_C64;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
+  for (long long i = (long long)bid * blockDim.x + threadIdx.x; i < n; i += (long long)nblk * blockDim.x)
     amp_put(st->amps, i, amp_get(st->amps, i, c64, r0, r1), c64);
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned done = atomicAdd(&c->sync_counter, 1u);
-    if (done == gridDim.x - 1) {
+    if (done == (unsigned)nblk - 1) {
       st->rscale[0] = ws.sel->kept;
       st->rscale[1] = 1.0;
       c->sync_counter = 0;
     }
   }
+}
+__global__ void k_materialize(bass_state* st, WsView ws, bass_ctrl* c) {
+  materialize_body(st, ws, c, blockIdx.x, gridDim.x);
+}
+__global__ void k_materialize_seg(const OpArgs* ops) {
+  const OpArgs& a = ops[blockIdx.y];
+  materialize_body(const_cast<bass_state*>(a.in), a.ws, a.ctrl, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -157,16 +185,15 @@ __global__ void k_fp_out(WsView ws, uint64_t* out6, bass_ctrl* c, int append, in
 // ---------------------------------------------------------------------------
 // sparse_state.py:178-190: a *= diag[(b_q1 << 1) | b_q2], in place
 template <bool C64>
-__global__ void k_phase2q(bass_state* st, double2 d0, double2 d1, double2 d2, double2 d3, int q1, int q2,
-                          bass_ctrl* c) {
+__device__ __forceinline__ void phase2q_body(bass_state* st, double2 d0, double2 d1, double2 d2, double2 d3, int q1,
+                                             int q2, bass_ctrl* c, int bid, int nblk) {
   const long long n = st->nnz;
   const int t1 = st->pos[q1], t2 = st->pos[q2];
   const double r0 = st->rscale[0], r1 = st->rscale[1];
   constexpr int c64 = C64;
   double* amps = st->amps;
   const uint64_t* keys = st->keys;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = (long long)bid * blockDim.x + threadIdx.x; i < n; i += (long long)nblk * blockDim.x) {
     const uint64_t y = keys[i];
     const int idx = (int)((((y >> t1) & 1ULL) << 1) | ((y >> t2) & 1ULL));
     const double2 d = idx == 0 ? d0 : idx == 1 ? d1 : idx == 2 ? d2 : d3;
@@ -177,7 +204,7 @@ __global__ void k_phase2q(bass_state* st, double2 d0, double2 d1, double2 d2, do
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned done = atomicAdd(&c->sync_counter, 1u);
-    if (done == gridDim.x - 1) {
+    if (done == (unsigned)nblk - 1) {
       st->rscale[0] = 1.0;
       st->rscale[1] = 1.0;
       c->amp_updates += n;
@@ -187,6 +214,20 @@ __global__ void k_phase2q(bass_state* st, double2 d0, double2 d1, double2 d2, do
       c->sync_counter = 0;
     }
   }
+}
+
+template <bool C64>
+__global__ void k_phase2q(bass_state* st, double2 d0, double2 d1, double2 d2, double2 d3, int q1, int q2,
+                          bass_ctrl* c) {
+  phase2q_body<C64>(st, d0, d1, d2, d3, q1, q2, c, blockIdx.x, gridDim.x);
+}
+
+// segmented: state blockIdx.y, diagonal G[0..3], qubits (q, j)
+template <bool C64>
+__global__ void k_phase2q_seg(const OpArgs* ops) {
+  const OpArgs& a = ops[blockIdx.y];
+  phase2q_body<C64>(const_cast<bass_state*>(a.in), a.G[0], a.G[1], a.G[2], a.G[3], a.q, a.j, a.ctrl, blockIdx.x,
+                    gridDim.x);
 }
 
 // 1-qubit diagonal gate: a = g_bb * a; children that are exactly zero are
@@ -802,6 +843,30 @@ cudaError_t run_renorm(bass_state* st, bass_ctrl* ctrl, const WsView& ws, cudaSt
   else KLAUNCH(S_REDUCE, s, k_reduce_state<R_NORM2, false><<<grid, 256, 0, s>>>(st, ws));
   KLAUNCH(S_REDUCE, s, k_renorm_apply<<<1, 256, 0, s>>>(st, ws, grid));
   KLAUNCH(S_SMALL, s, k_materialize<<<device().sms * 4, 256, 0, s>>>(st, ws, ctrl));
+  return cudaGetLastError();
+}
+
+cudaError_t run_phase2q_seg(const OpArgs* ops, int nseg, int c64, cudaStream_t s) {
+  const dim3 grid(device().sms, nseg);
+  if (c64) KLAUNCH(S_PHASE2Q, s, k_phase2q_seg<true><<<grid, 256, 0, s>>>(ops));
+  else KLAUNCH(S_PHASE2Q, s, k_phase2q_seg<false><<<grid, 256, 0, s>>>(ops));
+  return cudaGetLastError();
+}
+
+// mode 1: PR of every state (ctrl->pr_last); mode 0: renormalise every state
+cudaError_t run_reduce_seg(const OpArgs* ops, int nseg, int mode, int c64, cudaStream_t s) {
+  const int gx = 64;  // partials per state (ws.red holds 1024)
+  const dim3 grid(gx, nseg);
+  if (mode == 1) {
+    if (c64) KLAUNCH(S_REDUCE, s, k_reduce_state_seg<R_P2, true><<<grid, 256, 0, s>>>(ops));
+    else KLAUNCH(S_REDUCE, s, k_reduce_state_seg<R_P2, false><<<grid, 256, 0, s>>>(ops));
+    KLAUNCH(S_REDUCE, s, k_pr_final_seg<<<nseg, 256, 0, s>>>(ops, gx));
+  } else {
+    if (c64) KLAUNCH(S_REDUCE, s, k_reduce_state_seg<R_NORM2, true><<<grid, 256, 0, s>>>(ops));
+    else KLAUNCH(S_REDUCE, s, k_reduce_state_seg<R_NORM2, false><<<grid, 256, 0, s>>>(ops));
+    KLAUNCH(S_REDUCE, s, k_renorm_apply_seg<<<nseg, 256, 0, s>>>(ops, gx));
+    KLAUNCH(S_SMALL, s, k_materialize_seg<<<dim3(device().sms, nseg), 256, 0, s>>>(ops));
+  }
   return cudaGetLastError();
 }
 

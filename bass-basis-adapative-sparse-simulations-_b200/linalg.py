@@ -67,3 +67,30 @@ def eigh_numpy(rho):
     if np.linalg.det(V).real < 0:
         V[:, 1] *= -1
     return evals, V
+
+
+def eigh_2x2_many(r):
+    """eigh_2x2 of many 2x2 RDMs at once: r holds rows (rho00, rho11, Re rho01,
+    Im rho01); returns V as an (M, 2, 2) array.  The same IEEE operations as
+    eigh_2x2, element by element (numpy's sqrt is correctly rounded too)."""
+    r = np.asarray(r, dtype=np.float64).reshape(-1, 4)
+    a, d, br, bi = r[:, 0], r[:, 1], r[:, 2], r[:, 3]
+    b_sq = br * br + bi * bi
+    tau = (d - a) * 0.5
+    disc = np.sqrt(tau * tau + b_sq)
+    tdp = tau + disc
+    tdm = tau - disc
+    with np.errstate(divide="ignore", invalid="ignore"):
+        n0 = np.sqrt(b_sq + tdp * tdp)
+        n1 = np.sqrt(b_sq + tdm * tdm)
+        V = np.zeros((len(a), 2, 2), dtype=np.complex128)
+        V[:, 0, 0] = br / n0 + 1j * (bi / n0)
+        V[:, 1, 0] = tdp / n0
+        V[:, 0, 1] = br / n1 + 1j * (bi / n1)
+        V[:, 1, 1] = tdm / n1
+    diag = b_sq < 1e-28
+    keep = diag & (a >= d)
+    swap = diag & ~(a >= d)
+    V[keep] = np.eye(2)
+    V[swap] = np.array([[0.0, 1.0], [1.0, 0.0]])
+    return V

@@ -298,6 +298,50 @@ int bass_radix_sort_u64(uint64_t* keys, double* amps, int64_t n, int key_bits, v
 int bass_merge_sorted(uint64_t* keys, double* amps, int64_t n, int64_t* n_out, void* ws,
                       size_t ws_bytes, bass_ctrl* ctrl, void* stream);
 
+/* ---- batched (segmented) ops ------------------------------------------------------ */
+/* One op on each of n independent states in one set of launches: every
+   kernel's grid is split into one block group per state, sized by the
+   state's share of the work (each state gets at least one block), and each
+   group runs the single-state algorithm on its state (own descriptor,
+   control block and workspace).  This is the "segment offset" form of the
+   calls above: the host array describes the segments, the library copies it
+   into the batch workspace (bass_batch_ws_bytes) and launches once per pass
+   for all of them.  All states of one call must have the same amplitude type;
+   n <= 256 for ops that truncate or rotate (their selection keeps every block
+   of the grid resident).  No counterpart in the reference, whose simulators
+   run one state at a time. */
+typedef struct bass_seg_op {
+  bass_state* in;    /* input state (rotation step: the current state)         */
+  bass_state* tmp;   /* scratch state of 2-qubit ops; a rotation's candidate   */
+  bass_state* out;   /* output state                                          */
+  bass_ctrl* ctrl;   /* this state's control block                            */
+  void* ws;          /* this state's workspace                                */
+  size_t ws_bytes;
+  double G[32];      /* 2x2 (first 8 doubles) or 4x4 complex128, row-major     */
+  int32_t q1, q2;    /* gate qubits; a rotation step's qubit j is q1           */
+  bass_trunc tr;     /* truncation (rotation step: k = tr.k_keep)              */
+  double* rho;       /* RDM: 4 device doubles per qubit                        */
+  int32_t num_qubits;/* RDM: qubits of this state                              */
+  int32_t pad;
+} bass_seg_op;
+size_t bass_batch_ws_bytes(int max_ops);
+/* bass_gate_1q on every segment (sparse_state.py:15-67 + truncation) */
+int bass_gate_1q_batch(const bass_seg_op* host_ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream);
+/* bass_gate_2q on every segment (bass_simulator.py:292-354 + truncation) */
+int bass_gate_2q_batch(const bass_seg_op* host_ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream);
+/* bass_phase_2q on every segment (sparse_state.py:178-190); diag = G[0..7] */
+int bass_phase_2q_batch(const bass_seg_op* host_ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream);
+/* bass_topk on every segment (truncation.py:68-113) */
+int bass_topk_batch(const bass_seg_op* host_ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream);
+/* bass_rotate_step on every segment (bass_simulator.py:755-814), no trace */
+int bass_rotate_step_batch(const bass_seg_op* host_ops, int n, void* batch_ws, size_t batch_ws_bytes,
+                           void* stream);
+/* bass_rdm_1q on every segment (bass_simulator.py:441-470) */
+int bass_rdm_1q_batch(const bass_seg_op* host_ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream);
+/* bass_pr (mode 1) or bass_renorm (mode 0) on every segment (bass_simulator.py:574-578, 551-554) */
+int bass_pr_batch(const bass_seg_op* host_ops, int n, int mode, void* batch_ws, size_t batch_ws_bytes,
+                  void* stream);
+
 /* ---- instrumentation ------------------------------------------------------------ */
 /* Number of kernels this library has launched (process-wide). */
 int64_t bass_launch_count(void);
