@@ -10,8 +10,8 @@ fallback: constructing a simulator without the CUDA library or without a GPU
 raises.
 
 The directory name is not a Python identifier, so the package is imported
-under the name ``bass_b200`` (see ``load()`` in bench.py / tests/conftest.py,
-or INTEGRATION.md).
+under the name ``bass_b200`` by a file-location import of this directory's
+``__init__.py`` (as ``load_pkg()`` in bench.py and tests/conftest.py do).
 """
 from . import gates, circuits  # noqa: F401
 from .gates import (  # noqa: F401

@@ -2,10 +2,10 @@
 // memory.
 //
 // bass_rdm_1q needs a caller-allocated workspace.  Some callers cannot make
-// that allocation: code that runs while a CUDA stream is being captured into a
-// graph (cudaMalloc is not allowed there), host runtimes whose device memory is
-// owned by another allocator that hands out no scratch, and embeddings that may
-// only pass buffers they were given.  bass_rdm_1q_noalloc computes the same
+// that allocation: host runtimes whose device memory is owned by another
+// allocator that hands out no scratch, plugins and embeddings that may only
+// pass the buffers they were given, and code running at a point where it may
+// not call cudaMalloc (which synchronises the device).  bass_rdm_1q_noalloc computes the same
 // moments with its scratch in the file-scope array below instead.
 //
 // Limits and rules:

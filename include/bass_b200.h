@@ -257,9 +257,9 @@ int bass_dense_dot(const double* u, const double* v, int64_t n, double* out, bas
    state's entries of conj(psi[x]) a_x (psi: dense 2^nq complex128, device). */
 int bass_sparse_dot(const bass_state* st, const double* psi, int nq, double* out, bass_ctrl* ctrl, void* ws,
                     size_t ws_bytes, void* stream);
-/* bass_rdm_1q for callers that cannot allocate device memory (a stream being
-   captured into a CUDA graph, a host runtime that owns all device memory, an
-   embedding that may only pass the buffers it was given).  No counterpart in
+/* bass_rdm_1q for callers that cannot allocate device memory (a host runtime
+   that owns all device memory, a plugin or embedding that may only pass the
+   buffers it was given, code that may not call cudaMalloc at that point).  No counterpart in
    the reference.  The scratch is a static array inside the library (about
    4.8 MB, held on every GPU that loads the library until exit); the state may
    hold at most 2^20 entries (max_entries is the caller's bound on st->nnz;

@@ -1,9 +1,9 @@
 """bass_rdm_1q_noalloc: the RDM moments for callers that cannot allocate.
 
 Some callers of this library cannot allocate device memory when they need the
-moments -- a stream that is being captured into a CUDA graph forbids
-cudaMalloc, and some host runtimes own all device memory and only hand out the
-buffers of the state.  The entry point under test keeps its scratch in a static
+moments: host runtimes that own all device memory and only hand out the
+state's buffers, and plugins or embeddings that may only pass the buffers they
+were given.  The entry point under test keeps its scratch in a static
 array inside the library and must give exactly the same moments as
 bass_rdm_1q (same kernels, exact order-independent sums).  The file name makes
 pytest collect it last.
