@@ -6,6 +6,14 @@ random-k: numpy's seeded weighted choice), 1-qubit gates through
 SparseState.apply_gate.  The per-gate seed follows the same LCG
 (simulator.py:158).  gamma and nnz histories are recorded on the device and
 read once at the end; per-gate runtimes come from CUDA events.
+
+Random-k draws entries by their index, so the entry order matters there.  The
+reference's hash-table gate (bass_simulator.py:292-354) emits its output in
+first-occurrence order over the input entries (input order, then output
+index 0-3), and the weighted choice keeps the drawn order.  The device state
+is key-sorted, so in random-k mode that order is tracked on the host
+(``ht_order`` below, ``SparseState._set_order``) and the choice runs over the
+entries in it.
 """
 from __future__ import annotations
 
@@ -13,6 +21,32 @@ import numpy as np
 
 from . import _native as nat
 from .state import SparseState
+
+
+def ht_order(x, a, G, q1, q2):
+    """The output keys of apply_2qubit_gate_ht (bass_simulator.py:292-354) in
+    the order it emits them: input entries in their order, for each the
+    output indices 0-3 whose product G[out, in] * a is not exactly zero; a
+    key's position is that of its first occurrence."""
+    x = np.asarray(x, dtype=np.uint64)
+    a = np.asarray(a, dtype=np.complex128)
+    G = np.asarray(G, dtype=np.complex128)
+    if len(x) == 0:
+        return x.copy()
+    s1, s2 = np.uint64(q1), np.uint64(q2)
+    m1, m2 = np.uint64(1) << s1, np.uint64(1) << s2
+    one = np.uint64(1)
+    in_idx = (((x >> s1) & one) << one | ((x >> s2) & one)).astype(np.int64)
+    base = x & ~(m1 | m2)
+    keys = np.empty((len(x), 4), dtype=np.uint64)
+    live = np.empty((len(x), 4), dtype=bool)
+    for o in range(4):
+        keys[:, o] = base | (m1 if o >> 1 else np.uint64(0)) | (m2 if o & 1 else np.uint64(0))
+        prod = G[o, in_idx] * a
+        live[:, o] = (prod.real != 0.0) | (prod.imag != 0.0)
+    flat = keys[live]   # row-major: input order, then output index
+    u, first = np.unique(flat, return_index=True)
+    return u[np.argsort(first, kind="stable")]
 
 
 class FixedBasisSimulator:
@@ -27,8 +61,8 @@ class FixedBasisSimulator:
         self.max_nnz_factor = max_nnz_factor
 
     def _random_k_2q(self, state, cur_seed):
-        """simulator.py:177-196 with the entries in true-key order."""
-        x, a = state._exported()
+        """simulator.py:177-196, over the entries in the reference's order."""
+        x, a = state._in_order()
         probs = np.abs(a) ** 2
         total = np.sum(probs)
         np.random.seed(cur_seed)
@@ -63,7 +97,10 @@ class FixedBasisSimulator:
                 if topk:
                     state._apply_2q(gate.matrix, q1, q2, nat.trunc(self.k, self.k, 2, 1))
                 else:
+                    xin, ain = state._in_order()
+                    order = ht_order(xin, ain, gate.matrix, q1, q2)
                     state._apply_2q(gate.matrix, q1, q2, nat.NO_TRUNC)
+                    state._set_order(order)
                     if state.nnz > self.k:
                         self._random_k_2q(state, cur)
             else:

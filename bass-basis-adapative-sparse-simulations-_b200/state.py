@@ -2,10 +2,15 @@
 
 The state lives in device memory as a sorted array of (physical key,
 complex128 amplitude) plus a descriptor (include/bass_b200.h, bass_state).
-``x`` and ``alpha`` are read-only host copies (true keys sorted ascending and
-their amplitudes, nnz entries; the reference keeps capacity-length arrays
-whose first nnz entries are valid, so ``x[:nnz]`` works on both).  Reading
-``x``, ``alpha``, ``nnz`` or ``gamma`` synchronises the stream.
+``x`` and ``alpha`` are read-only host copies of the nnz entries (the
+reference keeps capacity-length arrays whose first nnz entries are valid, so
+``x[:nnz]`` works on both), in the reference's entry order: ascending true
+key after every gate (sparse_state.py:268-301 sorts), and the order of the
+drawn entries after a random-k truncation (truncation.py:116-159), of
+``load``, or of the hash-table gate of FixedBasisSimulator.  The device keeps
+the entries sorted by physical key; that order is tracked on the host, as the
+true keys in order, only while it differs from key order.  Reading ``x``,
+``alpha``, ``nnz`` or ``gamma`` synchronises the stream.
 """
 from __future__ import annotations
 
@@ -36,6 +41,7 @@ class SparseState:
         self._tmp2 = nat.DevState(self._eng, cap, 0, at)
         self._version = 0
         self._export = None
+        self._order = None   # the reference's entry order (true keys) when not ascending
 
     # ---- host views -----------------------------------------------------------
     def __repr__(self):
@@ -56,31 +62,63 @@ class SparseState:
         self._eng.set_ctrl("state_gamma", float(v))
 
     def _exported(self):
+        """The entries in ascending true-key order (host copies)."""
         if self._export is None or self._export[0] != self._version:
             self._eng.check_errors()
             x, a = self._cur.export()
-            self._export = (self._version, x, a)
+            self._export = (self._version, x, a, None)
         return self._export[1], self._export[2]
+
+    def _in_order(self):
+        """The entries in the reference's order (see the module docstring)."""
+        x, a = self._exported()
+        if self._order is None:
+            return x, a
+        if self._export[3] is None:
+            pos = np.searchsorted(x, self._order)
+            if len(self._order) != len(x) or not np.array_equal(x[np.minimum(pos, len(x) - 1)], self._order):
+                raise RuntimeError("entry order out of step with the device state")
+            self._export = self._export[:3] + ((self._order, a[pos]),)
+        return self._export[3]
 
     @property
     def x(self) -> np.ndarray:
-        return self._exported()[0]
+        return self._in_order()[0]
 
     @property
     def alpha(self) -> np.ndarray:
-        return self._exported()[1]
+        return self._in_order()[1]
 
     def _touch(self):
         self._version += 1
 
+    def _rekeyed(self):
+        """After an op whose result the reference holds in key order."""
+        self._touch()
+        self._order = None
+
+    def _set_order(self, keys):
+        """Record the reference's entry order (true keys, a permutation of
+        the state's keys); None or ascending keys mean key order."""
+        if keys is None:
+            self._order = None
+            return
+        keys = np.asarray(keys, dtype=np.uint64)
+        self._order = None if (len(keys) < 2 or bool(np.all(keys[1:] > keys[:-1]))) else keys.copy()
+        self._export = None if self._export is None else self._export[:3] + (None,)
+
     def load(self, x, alpha):
-        """Replace the entries (any order; duplicate keys are summed)."""
+        """Replace the entries (any order; duplicate keys are summed).  The
+        entries then read back in the given order (first occurrences)."""
+        x = np.asarray(x, dtype=np.uint64)
         self._cur.load(x, alpha)
         self._touch()
+        u, first = np.unique(x, return_index=True)
+        self._set_order(x if len(u) == len(x) else u[np.argsort(first)])
 
     def copy(self):
         new = SparseState(self.N, self.k, dtype=self.dtype, _capacity=self._cur.cap)
-        x, a = self._exported()
+        x, a = self._in_order()
         new.load(x, a)
         new.gamma = self.gamma
         return new
@@ -134,7 +172,7 @@ class SparseState:
             nat.check(eng.L.bass_gate_1q(self._cur.ptr, self._tmp.ptr, nat._host(g), int(q), tr, eng.ctrl_ptr,
                                          eng.ws_ptr, eng.ws_bytes, eng.stream), "bass_gate_1q")
             nat.swap(self._cur, self._tmp)
-        self._touch()
+        self._rekeyed()
 
     def _apply_2q(self, G, q1, q2, tr):
         eng = self._eng
@@ -143,7 +181,7 @@ class SparseState:
                                      int(q2), tr, eng.ctrl_ptr, eng.ws_ptr, eng.ws_bytes, eng.stream),
                   "bass_gate_2q")
         nat.swap(self._cur, self._tmp2)
-        self._touch()
+        self._rekeyed()
 
     def _rotate_2q(self, U4, q1, q2, tr):
         """bass_simulator.py:237-289 apply_2qubit_rotation_sparse with the
@@ -154,7 +192,7 @@ class SparseState:
                                        int(q2), tr, eng.ctrl_ptr, eng.ws_ptr, eng.ws_bytes, eng.stream),
                   "bass_rotate_2q")
         nat.swap(self._cur, self._tmp2)
-        self._touch()
+        self._rekeyed()
 
     def _rdm_2q(self, q1, q2) -> np.ndarray:
         """bass_simulator.py:200-231 compute_2qubit_rdm: 4x4 complex, index
@@ -190,7 +228,7 @@ class SparseState:
         nat.check(eng.L.bass_topk(self._cur.ptr, self._tmp.ptr, tr, eng.ctrl_ptr, eng.ws_ptr, eng.ws_bytes,
                                   eng.stream), "bass_topk")
         nat.swap(self._cur, self._tmp)
-        self._touch()
+        self._rekeyed()
 
     def _renorm(self, trace=0):
         eng = self._eng
@@ -219,7 +257,7 @@ class SparseState:
                                     eng.ctrl_ptr, eng.stream), "bass_gather")
         torch.cuda.current_stream(eng.device).synchronize()
         nat.swap(self._cur, self._tmp)
-        self._touch()
+        self._rekeyed()
 
     # ---- reference API ------------------------------------------------------------
     def apply_gate(self, gate, method="top-k", seed="None"):
@@ -248,16 +286,16 @@ class SparseState:
 
     def truncate_random_k(self, seed):
         """sparse_state.py:402-415 / truncation.py:116-159: the LCG partial
-        Fisher-Yates picks k entries by their index in the array.  The indices
-        refer to the entries in true-key order, which is the reference's own
-        order whenever its array is key-sorted (after any non-truncating
-        gate).  Host-driven: export, choose, re-import."""
+        Fisher-Yates picks k entries by their index in the array, in the
+        reference's entry order (key order after a gate, the drawn order after
+        an earlier random-k truncation); the drawn entries keep the order of
+        the draw.  Host-driven: export, choose, re-import."""
         n = self.nnz
         if n <= self.k:
             return
         if seed is None:
             seed = int(np.random.randint(0, 2 ** 31))
-        x, a = self._exported()
+        x, a = self._in_order()
         idx = np.empty(self.k, dtype=np.int64)
         nat.check(self._eng.L.bass_lcg_choose(n, self.k, int(seed), nat._host(idx)), "bass_lcg_choose")
         self.load(x[idx], a[idx])
