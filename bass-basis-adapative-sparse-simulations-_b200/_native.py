@@ -53,8 +53,15 @@ KINDS = ["gate1", "rot1", "gate2", "perm", "plain", "rdm"]
 PASSES = ["hist", "hist2", "gather", "write", "rdm"]
 SLOT_NAMES = [f"k_tile<{k},{p}>" for k in KINDS for p in PASSES] + [
     "k_partition", "k_select_coop", "k_select2", "k_tie_coop", "k_finalize", "reductions", "k_fingerprint",
-    "k_phase2q", "k_phase1q", "k_rdm_final", "radix_sort", "merge_runs", "bookkeeping", "k_slot_hist<1>",
-    "k_slot_hist<2>", "k_slot_gather", "k_tile_counts"] + [f"slot{i}" for i in range(47, 48)]
+    "k_phase2q", "k_phase1q", "k_rdm_final", "radix_sort", "merge_runs", "bookkeeping", "select:level1",
+    "select:level2", "select:count", "select:settle+final", "select:two_level"]
+# select:* slots hold nanoseconds of k_select_coop's phases (block 0's clock,
+# barrier waits included; the last block's for settle+final) in prof_in and the
+# number of timed launches in prof_out; two_level counts (in prof_in) the
+# selections whose threshold needed the level-2 histogram, out of all
+# truncating selections (prof_out)
+SELECT_PHASE_SLOTS = (43, 44, 45, 46)
+SELECT_SPEC_SLOT = 47
 # the write step of gates, rotations and truncations is k_compact, counted in the write slot
 SLOT_NAMES[0 * 5 + 3] = "k_compact<gate1>"
 SLOT_NAMES[1 * 5 + 3] = "k_compact<rot1>"

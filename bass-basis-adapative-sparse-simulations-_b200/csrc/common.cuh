@@ -376,6 +376,12 @@ __device__ __forceinline__ void warp_lower_bound3(const uint64_t* keys, long lon
 // this block's part of the grid no longer needs its SM to itself, so the next
 // kernel may be scheduled.  Both are no-ops for a kernel launched normally.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Nanosecond wall clock of the GPU (profiling of phases inside one launch).
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // One galloping round before warp_lower_bound3, for three searches whose
@@ -534,7 +540,7 @@ struct Partial {
 struct SelState {
   long long n_out;       // children produced by the op (after drop rules)
   long long k_keep;
-  long long n_cand;      // children of the level-2 boundary bin collected by the count pass
+  long long n_cand;      // children of the level-2 boundary bin (slot indices in ws.cand_bits)
   unsigned long long t_bits;
   unsigned long long t_key;  // ~0: every child at t_bits kept; else the largest kept true key there
   int do_trunc;
@@ -556,7 +562,7 @@ struct WsView {
   unsigned int* hist1;           // kHistBins bins, then kHistGroups coarse counts
   unsigned int* hist2;           // kHistBins bins, then kHistGroups coarse counts
   Partial* partials;             // kMaxSets x max_tiles
-  unsigned long long* cand_bits; // max_n
+  unsigned long long* cand_bits; // max_n: slot indices (boundary-bin candidates of a selection)
   unsigned long long* cand_key;  // max_n
   SelState* sel;
   unsigned int* counters;        // 64 tile counters

@@ -984,6 +984,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
 // barrier is a counter and a generation word in the
 // workspace with a bounded spin (BASS_ERR_WAIT, then every block returns).
 constexpr int kSelThreads = 512;
+// dynamic shared memory of the selection: the histograms (kHistBins words),
+// later the boundary candidates (bits, true key, slot index)
+constexpr size_t kSelSmem = (size_t)kCandSmem * 24;
 
 // Grid-wide barrier of the selection's grid (every block resident, see
 // launch_select_t).  Returns false (error recorded) if the wait gave up.
@@ -1083,6 +1086,23 @@ __device__ int find_bin(const unsigned int* hist, long long k, long long* c_gt, 
   return sRes;
 }
 
+// Adds the block's shared histogram h into the global histogram gh and its
+// coarse counts of 64 groups of 128 bins (gh[kHistBins + g]), for find_bin.
+__device__ void flush_hist(const unsigned int* h, unsigned int* gh) {
+  for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
+    if (h[i]) atomicAdd(&gh[i], h[i]);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int g = w; g < kHistGroups; g += nw) {
+    const unsigned* hg = h + g * kGroupBins;
+    unsigned c = 0;
+#pragma unroll
+    for (int q = 0; q < kGroupBins / 32; ++q) c += hg[32 * q + lane];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+    if (lane == 0 && c) atomicAdd(&gh[kHistBins + g], c);
+  }
+}
+
 // Block-wide histogram of the slots (LEVEL 1: bits >> 50; LEVEL 2: bits
 // 37-49 of the slots whose bits >> 50 equal pre), added into gh.
 template <int LEVEL>
@@ -1121,19 +1141,7 @@ __device__ void slot_hist_phase(const unsigned long long* slots, long long nslot
     if (valid) atomicAdd(&h[bin], 1u);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
-    if (h[i]) atomicAdd(&gh[i], h[i]);
-  // coarse counts of 64 groups of 128 bins (gh[kHistBins + g]), for find_bin
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int g = w; g < kHistGroups; g += nw) {
-    const unsigned* hg = h + g * kGroupBins;
-    unsigned c = 0;
-#pragma unroll
-    for (int q = 0; q < kGroupBins / 32; ++q) c += hg[32 * q + lane];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
-    if (lane == 0 && c) atomicAdd(&gh[kHistBins + g], c);
-  }
+  flush_hist(h, gh);
 }
 
 // better(a, b): a ranks strictly above b
@@ -1142,15 +1150,17 @@ __device__ __forceinline__ bool better(unsigned long long ab, unsigned long long
   return ab > bb || (ab == bb && ak < bk);
 }
 
-// Sorts sb / sk [0, m) (m <= kCandSmem) by (bits desc, key asc): bitonic,
-// padded to a power of two with pairs that rank below every candidate.
-__device__ void sort_pairs(unsigned long long* sb, unsigned long long* sk, long long m) {
+// Sorts sb / sk [0, m) (m <= kCandSmem) by (bits desc, key asc), moving si
+// along: bitonic, padded to a power of two with pairs that rank below every
+// candidate.
+__device__ void sort_pairs(unsigned long long* sb, unsigned long long* sk, unsigned long long* si, long long m) {
   const int tid = threadIdx.x;
   int P = 1;
   while (P < m) P <<= 1;
   for (int i = tid + (int)m; i < P; i += blockDim.x) {
     sb[i] = 0;
     sk[i] = ~0ULL;
+    si[i] = 0;
   }
   __syncthreads();
   for (int size = 2; size <= P; size <<= 1) {
@@ -1161,8 +1171,8 @@ __device__ void sort_pairs(unsigned long long* sb, unsigned long long* sk, long 
           const bool up = (i & size) == 0;
           const bool sw = up ? better(sb[jx], sk[jx], sb[i], sk[i]) : better(sb[i], sk[i], sb[jx], sk[jx]);
           if (sw) {
-            unsigned long long tb = sb[i], tk = sk[i];
-            sb[i] = sb[jx]; sk[i] = sk[jx]; sb[jx] = tb; sk[jx] = tk;
+            unsigned long long tb = sb[i], tk = sk[i], ti = si[i];
+            sb[i] = sb[jx]; sk[i] = sk[jx]; si[i] = si[jx]; sb[jx] = tb; sk[jx] = tk; si[jx] = ti;
           }
         }
       }
@@ -1171,20 +1181,29 @@ __device__ void sort_pairs(unsigned long long* sb, unsigned long long* sk, long 
   }
 }
 
-// The threshold of the level-2 boundary bin's m candidates (slot index in
-// ws.cand_bits, true key in ws.cand_key; m <= kCandSmem), one block: the
-// need-th best child by (bits desc, key asc) gives (t_bits, t_key); t_key is
-// ~0 when every candidate at t_bits is kept.  Every block of the selection
-// runs it on the same candidates and reaches the same pair.
-__device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, long long need,
+// The true key of the child staged at slot i (qat: the op's output order).
+__device__ __forceinline__ unsigned long long cand_true_key(const OpArgs& a, unsigned long long i,
+                                                            const int8_t* qat) {
+  return true_key(__ldcg(a.ws.stage_keys + i), qat, 64);
+}
+
+// The threshold of the level-2 boundary bin's m candidates (slot indices in
+// ws.cand_bits; m <= kCandSmem), one block: the need-th best child by (bits
+// desc, true key asc) gives (t_bits, t_key); t_key is ~0 when every candidate
+// at t_bits is kept.  The candidates stay in shared memory (bits, true key,
+// slot index: three arrays of kCandSmem words, in some order) for the caller.
+__device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, long long need, const int8_t* qat,
                              unsigned long long* tb_out, unsigned long long* tk_out) {
   unsigned long long* sb = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* sk = sb + kCandSmem;
+  unsigned long long* ssi = sk + kCandSmem;
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
   const int tid = threadIdx.x;
   for (long long i = tid; i < m; i += blockDim.x) {
-    sb[i] = __ldcg(slots + __ldcg(a.ws.cand_bits + i));
-    sk[i] = __ldcg(a.ws.cand_key + i);
+    const unsigned long long si = __ldcg(a.ws.cand_bits + i);
+    ssi[i] = si;
+    sb[i] = __ldcg(slots + si);
+    sk[i] = cand_true_key(a, si, qat);
   }
   __syncthreads();
   const long long r = need < 1 ? 0 : (need > m ? m - 1 : need - 1);
@@ -1199,7 +1218,7 @@ __device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, 
       if (rank == r) sSel = (int)i;
     }
   } else {
-    sort_pairs(sb, sk, m);
+    sort_pairs(sb, sk, ssi, m);
     if (tid == 0) sSel = (int)r;
   }
   __syncthreads();
@@ -1209,14 +1228,15 @@ __device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, 
   __syncthreads();
   *tb_out = tb;
   *tk_out = sCut ? tk : ~0ULL;
-  __syncthreads();  // smem is reused by the caller
+  __syncthreads();
 }
 
-// The same threshold for m > kCandSmem (block 0 alone): radix select on the
+// The same threshold for m > kCandSmem (one block): radix select on the
 // low 37 bits of the bit pattern (the 26-bit prefix pre is shared), then, if
 // the cut falls inside a run of equal patterns, on the true keys of that run.
 __device__ void settle_radix(const OpArgs& a, unsigned char* smem, long long m, long long need,
-                             unsigned long long pre, unsigned long long* tb_out, unsigned long long* tk_out) {
+                             unsigned long long pre, const int8_t* qat, unsigned long long* tb_out,
+                             unsigned long long* tk_out) {
   unsigned int* h = reinterpret_cast<unsigned int*>(smem);
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
   const int tid = threadIdx.x;
@@ -1262,8 +1282,9 @@ __device__ void settle_radix(const OpArgs& a, unsigned char* smem, long long m, 
     __syncthreads();
     const unsigned long long p = sKeyPre;
     for (long long i = tid; i < m; i += blockDim.x) {
-      if (__ldcg(slots + __ldcg(a.ws.cand_bits + i)) != tb) continue;
-      const unsigned long long k = __ldcg(a.ws.cand_key + i);
+      const unsigned long long si = __ldcg(a.ws.cand_bits + i);
+      if (__ldcg(slots + si) != tb) continue;
+      const unsigned long long k = cand_true_key(a, si, qat);
       if (shift == 56 || (k >> (shift + 8)) == p) atomicAdd(&h[(unsigned)(k >> shift) & 255u], 1u);
     }
     __syncthreads();
@@ -1301,10 +1322,11 @@ __device__ __forceinline__ long long tile_of(long long z, int kind, const long l
 // tile) and, per CTA in partials s[0..2], the exact mass of the survivors,
 // their sum of |a|^4 (P2) and the exact mass of all children (when
 // truncating).  cand: the children of the level-2 boundary bin (bits >> 37 ==
-// cpre, all below T) are collected for settle_small / settle_radix as well.
+// cpre, all below T) are listed as well (slot indices in ws.cand_bits,
+// counted in sel->n_cand), for settle_boundary.
 template <bool P2>
 __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long long T, bool incl, bool trunc,
-                            i128* sRed, bool cand, unsigned long long cpre, const int8_t* qat, Grp g) {
+                            i128* sRed, bool cand, unsigned long long cpre, Grp g) {
   const long long n = a.in->nnz;
   const long long nslots = (long long)ns * n;
   const bool sums = P2 || trunc;
@@ -1316,10 +1338,9 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
   i128 v[3] = {0, 0, 0};
   const long long nchunk = (nslots + 7) >> 3;
   const long long stride = (long long)g.nblk * blockDim.x;
-  for (long long cb = (long long)g.bid * blockDim.x + (threadIdx.x & ~31); cb < nchunk; cb += stride) {
-    const long long c = cb + lane;  // this thread's chunk: slots [8c, 8c + 8)
+  // the thread's chunk of slots [8c, 8c + 8)
+  auto load_chunk = [&](long long c, unsigned long long* x) {
     const long long s0 = c << 3;
-    unsigned long long x[8];
     if (s0 + 8 <= nslots) {
       const ulonglong2* q = reinterpret_cast<const ulonglong2*>(slots + s0);
 #pragma unroll
@@ -1332,9 +1353,15 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
 #pragma unroll
       for (int u = 0; u < 8; ++u) x[u] = (s0 + u < nslots) ? slots[s0 + u] : ~0ULL;
     }
+  };
+  for (long long cb = (long long)g.bid * blockDim.x + (threadIdx.x & ~31); cb < nchunk; cb += stride) {
+    const long long c = cb + lane;  // this thread's chunk: slots [8c, 8c + 8)
+    const long long s0 = c << 3;
+    unsigned long long x[8];
+    load_chunk(c, x);
     if (cand) {
-      // the boundary bin's children: appended (slot, true key) to the
-      // candidate arrays, one atomic per warp
+      // the boundary bin's children: slot indices appended to the list, one
+      // atomic per warp
       unsigned cm = 0;
 #pragma unroll
       for (int u = 0; u < 8; ++u) cm |= (unsigned)(x[u] != ~0ULL && (x[u] >> 37) == cpre) << u;
@@ -1353,10 +1380,7 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
         long long k = (long long)base + inc - cc;
         for (int u = 0; u < 8; ++u) {
           if (!((cm >> u) & 1u)) continue;
-          if (k < a.ws.max_n) {
-            a.ws.cand_bits[k] = (unsigned long long)(s0 + u);
-            a.ws.cand_key[k] = true_key(a.ws.stage_keys[s0 + u], qat, 64);
-          }
+          if (k < a.ws.max_n) a.ws.cand_bits[k] = (unsigned long long)(s0 + u);
           ++k;
         }
       }
@@ -1431,14 +1455,65 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
   }
 }
 
+// The boundary bin of a selection whose threshold lies inside its level-2
+// bin (late): its m children (slot indices in ws.cand_bits, collected by
+// the count pass) are below every kept child of the other bins.  Run by one
+// block (the last to finish): the need-th best of them by (bits desc, true
+// key asc) gives (t_bits, t_key); the kept ones are added to their tiles'
+// counts and to this thread's share of the kept mass (vk[0]) and sum of
+// |a|^4 (vk[1]).  qat: the op's output order (for the true keys).
+template <bool P2>
+__device__ void settle_boundary(const OpArgs& a, int ns, int kind, unsigned long long lpre, long long lneed,
+                                const int8_t* qat, i128* vk) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long sM;
+  SelState* sel = a.ws.sel;
+  const int tid = threadIdx.x;
+  if (tid == 0) sM = *(volatile long long*)&sel->n_cand;
+  __syncthreads();
+  long long m = sM;
+  if (m > a.ws.max_n) {
+    if (tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+    m = a.ws.max_n;
+  }
+  unsigned long long tb, tk;
+  if (m <= kCandSmem) settle_small(a, smem, m, lneed, qat, &tb, &tk);
+  else settle_radix(a, smem, m, lneed, lpre, qat, &tb, &tk);
+  if (tid == 0) {
+    sel->t_bits = tb;
+    sel->t_key = tk;
+  }
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;
+  const bool in_smem = m <= kCandSmem;  // settle_small left (bits, key, slot) there
+  const unsigned long long* sb = reinterpret_cast<const unsigned long long*>(smem);
+  for (long long k = tid; k < m; k += blockDim.x) {
+    const unsigned long long i = in_smem ? sb[2 * kCandSmem + k] : __ldcg(a.ws.cand_bits + k);
+    const unsigned long long bits = in_smem ? sb[k] : __ldcg(slots + i);
+    if (bits > tb || (bits == tb && (in_smem ? sb[kCandSmem + k] : cand_true_key(a, i, qat)) <= tk)) {
+      atomicAdd(reinterpret_cast<unsigned long long*>(a.ws.status + tile_of((long long)(i >> lns), kind, a.ws.part)),
+                1ULL);
+      vk[0] += fx_from_pbits(bits);
+      if (P2) {
+        const double p = __longlong_as_double((long long)bits);
+        vk[1] += fx_from_pbits((unsigned long long)__double_as_longlong(__dmul_rn(p, p)));
+      }
+    }
+  }
+  __threadfence();
+  __syncthreads();
+}
+
 // The last block after the counts: exact kept / total mass (tied children added
-// back), the rotation decision (mode 1, the rule of bass_simulator.py:795-814:
-// the candidate's PR = kept^2 / sum |a|^4 against ctrl->pr_cur; a rejected
-// candidate is not written unless a trace is kept), and the exclusive scan of
-// the tile counts in ws.status.
-__device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j, int trace, i128* sRed) {
+// back: vk, this thread's share of the settled boundary bin), the rotation
+// decision (mode 1, the rule of bass_simulator.py:795-814: the candidate's PR
+// = kept^2 / sum |a|^4 against ctrl->pr_cur; a rejected candidate is not
+// written unless a trace is kept), and the exclusive scan of the tile counts
+// in ws.status.
+__device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j, int trace, i128* sRed,
+                            const i128* vk) {
   volatile SelState* sel = a.ws.sel;  // written by other blocks of this kernel
-  i128 v[3] = {0, 0, 0};
+  i128 v[3] = {vk[0], vk[1], 0};
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
     const Partial* p = a.ws.partials + b;
     v[0] += (i128)(((u128)__ldcg((const unsigned long long*)&p->s[0] + 1) << 64) |
@@ -1468,41 +1543,60 @@ __device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j
       sel->skip_write = (reject && !trace) ? 1 : 0;
     }
   }
-  // exclusive scan of the per-tile counts, in coalesced rounds of blockDim
+  // exclusive scan of the per-tile counts: every thread owns a contiguous run
+  // of C tiles (all its loads issued at once), one block scan of the run sums
   __shared__ long long sW[32];
   __shared__ long long sCarry;
   const long long n = a.in->nnz;
   const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
   const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
-  if (t == 0) sCarry = 0;
+  const long long C = (ntiles + blockDim.x - 1) / blockDim.x;
+  const long long lo = (long long)t * C;
+  const long long hi = lo + C < ntiles ? lo + C : ntiles;
+  constexpr int kRun = 8;
+  long long cr[kRun];
+  long long run = 0;
+  if (C <= kRun) {
+#pragma unroll
+    for (int q = 0; q < kRun; ++q) {
+      cr[q] = (lo + q < hi) ? (long long)__ldcg(a.ws.status + lo + q) : 0;
+      run += cr[q];
+    }
+  } else {
+    for (long long b = lo; b < hi; ++b) run += (long long)__ldcg(a.ws.status + b);
+  }
+  long long x = run;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) sW[w] = x;
   __syncthreads();
-  for (long long r0 = 0; r0 < ntiles; r0 += blockDim.x) {
-    const long long b = r0 + t;
-    const long long c = (b < ntiles) ? (long long)__ldcg(a.ws.status + b) : 0;
-    long long x = c;
+  if (w == 0) {
+    long long y = (lane < nw) ? sW[lane] : 0;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const long long y = __shfl_up_sync(0xffffffffu, x, off);
-      if (lane >= off) x += y;
+      const long long z = __shfl_up_sync(0xffffffffu, y, off);
+      if (lane >= off) y += z;
     }
-    if (lane == 31) sW[w] = x;
-    __syncthreads();
-    if (w == 0) {
-      long long y = (lane < nw) ? sW[lane] : 0;
+    if (lane < nw) sW[lane] = y;
+    if (lane == nw - 1) sCarry = y;
+  }
+  __syncthreads();
+  long long ex = x - run + (w > 0 ? sW[w - 1] : 0);
+  if (C <= kRun) {
 #pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const long long z = __shfl_up_sync(0xffffffffu, y, off);
-        if (lane >= off) y += z;
-      }
-      if (lane < nw) sW[lane] = y;
+    for (int q = 0; q < kRun; ++q) {
+      if (lo + q < hi) a.ws.status[lo + q] = (unsigned long long)ex;
+      ex += cr[q];
     }
-    __syncthreads();
-    const long long carry = sCarry;
-    const long long incl = x + (w > 0 ? sW[w - 1] : 0);
-    if (b < ntiles) a.ws.status[b] = (unsigned long long)(carry + incl - c);
-    __syncthreads();
-    if (t == blockDim.x - 1) sCarry = carry + incl;
-    __syncthreads();
+  } else {
+    for (long long b = lo; b < hi; ++b) {
+      const long long c = (long long)__ldcg(a.ws.status + b);
+      a.ws.status[b] = (unsigned long long)ex;
+      ex += c;
+    }
   }
   if (t == 0) {
     sel->n_written = sCarry;
@@ -1510,9 +1604,12 @@ __device__ void final_phase(const OpArgs& a, int nblk, int kind, int mode, int j
   }
 }
 
-// After count_phase: the last block to finish runs final_phase (the others
-// exit), which needs every block's partial sums and tile counts.
-__device__ void finish_by_last_block(const OpArgs& a, int kind, int mode, int j, int trace, i128* sRed, Grp g) {
+// After count_phase: the last block to finish settles the boundary bin (if
+// late) and runs final_phase (the others exit), which needs every block's
+// partial sums and tile counts.
+template <bool P2>
+__device__ void finish_by_last_block(const OpArgs& a, int ns, int kind, int mode, int j, int trace, i128* sRed,
+                                     Grp g, bool late, unsigned long long lpre, long long lneed, const int8_t* qat) {
   __shared__ int sLast;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1522,7 +1619,17 @@ __device__ void finish_by_last_block(const OpArgs& a, int kind, int mode, int j,
     __threadfence();
   }
   __syncthreads();
-  if (sLast) final_phase(a, g.nblk, kind, mode, j, trace, sRed);
+  if (!sLast) return;
+  const unsigned long long t0 = a.prof ? gtimer() : 0ULL;
+  i128 vk[2] = {0, 0};
+  if (late) settle_boundary<P2>(a, ns, kind, lpre, lneed, qat, vk);
+  final_phase(a, g.nblk, kind, mode, j, trace, sRed, vk);
+  if (a.prof && threadIdx.x == 0 && a.ws.sel->do_trunc) {
+    unsigned long long* pin = reinterpret_cast<unsigned long long*>(a.ctrl->prof_in);
+    unsigned long long* pout = reinterpret_cast<unsigned long long*>(a.ctrl->prof_out);
+    atomicAdd(pin + S_SLOT_KEPT, gtimer() - t0);
+    atomicAdd(pout + S_SLOT_KEPT, 1ULL);
+  }
 }
 
 template <bool P2>
@@ -1533,6 +1640,7 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
   __shared__ long long sS[kSelThreads / 32];
   __shared__ i128 sRed[3 * (kSelThreads / 32)];
   __shared__ long long sNout;
+  __shared__ int8_t sQat[64];
   SelState* sel = a.ws.sel;
   const int tid = threadIdx.x;
   const long long n = a.in->nnz;
@@ -1543,6 +1651,12 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
     return;
   }
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  // profiling: block 0 times its phases (level 1, level 2, count pass),
+  // barrier waits included; the last block times the boundary settle and the
+  // final phase
+  const bool ptime = a.prof && g.bid == 0 && tid == 0;
+  unsigned long long tp[4] = {0, 0, 0, 0};
+  if (ptime) tp[0] = gtimer();
   // 1. the child count
   long long cn = 0;
   for (int b = tid; b < nblk_hist; b += blockDim.x) cn += __ldcg(&a.ws.partials[b].c[0]);
@@ -1560,9 +1674,10 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
   const bool trunc = !(a.k_cond < 0 || n_out <= a.k_cond || a.k_keep >= n_out);
   unsigned long long T = 0ULL, tkey = ~0ULL;
   bool incl = true;
-  bool late = false;  // the threshold lies inside the level-2 bin lpre
+  bool late = false;  // the threshold lies inside the level-2 bin lpre: settled by the last block
   unsigned long long lpre = 0;
   long long lneed = 0;
+  int two = 0;        // a level-2 pass was needed
   if (trunc && a.k_keep <= 0) {
     T = ~0ULL;
     tkey = 0ULL;
@@ -1574,9 +1689,11 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
     long long c_gt, c_b1;
     const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, &c_b1);
     const long long need = a.k_keep - c_gt;
+    if (ptime) tp[1] = gtimer();
     if (c_b1 == need) {
       T = (unsigned long long)b1 << 50;
     } else {
+      two = 1;
       slot_hist_phase<2>(slots, nslots, (unsigned long long)b1, h, a.ws.hist2, g);
       if (!grid_sync(a, g)) return;
       long long c_gt2, c_b2;
@@ -1587,7 +1704,7 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
         T = pre << 37;
       } else {
         // the bin's children are settled after the count pass, which keeps
-        // everything above the bin and collects the bin itself
+        // everything above the bin and lists the bin itself
         late = true;
         lpre = pre;
         lneed = need2;
@@ -1603,76 +1720,29 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
     sel->t_bits = T;
     sel->t_key = tkey;
   }
-  __shared__ int8_t sQat[64];
   if (late) {
     out_order_par(a.in, kind, a.q, a.gb, sQat);
     __syncthreads();
     if (g.bid == 0 && tid < 64) sel->qat[tid] = sQat[tid];
   }
   // 3. survivors per tile and exact sums
-  count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, late, lpre, sQat, g);
-  if (late) {
-    // 3b. the boundary bin: its threshold pair, then its survivors counted
-    // per tile and their mass added to this block's partial sums
-    if (!grid_sync(a, g)) return;
-    __shared__ long long sM;
-    __shared__ unsigned long long sTb, sTk;
-    if (tid == 0) sM = *(volatile long long*)&sel->n_cand;
-    __syncthreads();
-    long long m = sM;
-    if (m > a.ws.max_n) {
-      if (g.bid == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
-      m = a.ws.max_n;
+  if (ptime) tp[2] = gtimer();
+  count_phase<P2>(a, ns, kind, trunc ? T : 0ULL, incl, trunc, sRed, late, lpre, g);
+  if (ptime && trunc) {
+    tp[3] = gtimer();
+    if (!tp[1]) tp[1] = tp[0];
+    unsigned long long* pin = reinterpret_cast<unsigned long long*>(a.ctrl->prof_in);
+    unsigned long long* pout = reinterpret_cast<unsigned long long*>(a.ctrl->prof_out);
+    for (int q = 0; q < 3; ++q) {
+      atomicAdd(pin + S_SLOT_HIST1 + q, tp[q + 1] - tp[q]);
+      atomicAdd(pout + S_SLOT_HIST1 + q, 1ULL);
     }
-    unsigned long long tb, tk;
-    if (m <= kCandSmem) {
-      settle_small(a, smem, m, lneed, &tb, &tk);
-    } else {
-      if (g.bid == 0) {
-        settle_radix(a, smem, m, lneed, lpre, &tb, &tk);
-        if (tid == 0) {
-          sel->t_bits = tb;
-          sel->t_key = tk;
-        }
-      }
-      if (!grid_sync(a, g)) return;
-      if (tid == 0) {
-        sTb = *(volatile unsigned long long*)&sel->t_bits;
-        sTk = *(volatile unsigned long long*)&sel->t_key;
-      }
-      __syncthreads();
-      tb = sTb;
-      tk = sTk;
-    }
-    if (g.bid == 0 && tid == 0) {
-      sel->t_bits = tb;
-      sel->t_key = tk;
-    }
-    const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;
-    i128 v[3] = {0, 0, 0};
-    for (long long k = (long long)g.bid * blockDim.x + tid; k < m; k += (long long)g.nblk * blockDim.x) {
-      const unsigned long long i = __ldcg(a.ws.cand_bits + k);
-      const unsigned long long bits = __ldcg(slots + i);
-      if (bits > tb || (bits == tb && __ldcg(a.ws.cand_key + k) <= tk)) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(a.ws.status + tile_of((long long)(i >> lns), kind, a.ws.part)),
-                  1ULL);
-        v[0] += fx_from_pbits(bits);
-        if (P2) {
-          const double p = __longlong_as_double((long long)bits);
-          v[1] += fx_from_pbits((unsigned long long)__double_as_longlong(__dmul_rn(p, p)));
-        }
-      }
-    }
-    block_sum_i128<3>(v, sRed);
-    if (tid == 0) {
-      Partial* pt = a.ws.partials + g.bid;
-      pt->s[0] += v[0];
-      pt->s[1] += v[1];
-    }
+    atomicAdd(pin + S_SLOT_KEPT + 1, (unsigned long long)two);
+    atomicAdd(pout + S_SLOT_KEPT + 1, 1ULL);
   }
-  // 4. sums, decision, tile offsets
+  // 4. boundary bin, sums, decision, tile offsets
   pdl_trigger();
-  finish_by_last_block(a, kind, mode, j, trace, sRed, g);
+  finish_by_last_block<P2>(a, ns, kind, mode, j, trace, sRed, g, late, lpre, lneed, sQat);
 }
 
 // nblk_hist: CTAs of the evaluation pass (per-CTA child counts in partials c[0]).
@@ -1942,7 +2012,7 @@ static cudaError_t launch_coop(void (*kern)(K...), dim3 grid, dim3 block, size_t
 template <bool P2>
 static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace,
                                    cudaStream_t s) {
-  const size_t smem = (size_t)kCandSmem * 16;
+  const size_t smem = kSelSmem;
   static int grid = 0;
   if (grid == 0) {
     const void* f = (const void*)k_select_coop<P2>;
@@ -2278,7 +2348,7 @@ static cudaError_t merge_op_seg(const OpArgs* ops, int nseg, int fin_mode, int t
   KLAUNCH(KIND * 5 + PASS, s, k_tile_seg<KIND, PASS, C64><<<gt, kThreads, smem, s>>>(ops, plan));
   if (KIND == K_PERM) return cudaGetLastError();
   constexpr int ns = slots_per_entry(KIND);
-  const size_t ssmem = (size_t)kCandSmem * 16;
+  const size_t ssmem = kSelSmem;
   cudaError_t e = cudaSuccess;
   if (fin_mode == 1) {
     static int gs1 = 0;

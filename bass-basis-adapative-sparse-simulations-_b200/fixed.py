@@ -69,7 +69,7 @@ class FixedBasisSimulator:
         pn = probs / total if total > 1e-30 else np.ones(len(a)) / len(a)
         idx = np.random.choice(len(a), size=self.k, replace=False, p=pn)
         kept = np.sum(probs[idx])
-        state.load(x[idx], a[idx])
+        state._load_in_order(x[idx], a[idx])
         state.gamma = state.gamma * (np.sqrt(kept / total) if total > 1e-30 else 0)
         state._renorm()
 

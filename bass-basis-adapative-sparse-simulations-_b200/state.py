@@ -6,8 +6,8 @@ complex128 amplitude) plus a descriptor (include/bass_b200.h, bass_state).
 reference keeps capacity-length arrays whose first nnz entries are valid, so
 ``x[:nnz]`` works on both), in the reference's entry order: ascending true
 key after every gate (sparse_state.py:268-301 sorts), and the order of the
-drawn entries after a random-k truncation (truncation.py:116-159), of
-``load``, or of the hash-table gate of FixedBasisSimulator.  The device keeps
+drawn entries after a random-k truncation (truncation.py:116-159), and the
+hash-table gate's order in FixedBasisSimulator.  The device keeps
 the entries sorted by physical key; that order is tracked on the host, as the
 true keys in order, only while it differs from key order.  Reading ``x``,
 ``alpha``, ``nnz`` or ``gamma`` synchronises the stream.
@@ -108,18 +108,23 @@ class SparseState:
         self._export = None if self._export is None else self._export[:3] + (None,)
 
     def load(self, x, alpha):
-        """Replace the entries (any order; duplicate keys are summed).  The
-        entries then read back in the given order (first occurrences)."""
+        """Replace the entries (any order; duplicate keys are summed); they
+        read back in ascending key order."""
+        self._cur.load(x, alpha)
+        self._rekeyed()
+
+    def _load_in_order(self, x, alpha):
+        """load() of distinct keys that then read back in the given order (the
+        reference's arrays after a random-k draw)."""
         x = np.asarray(x, dtype=np.uint64)
         self._cur.load(x, alpha)
         self._touch()
-        u, first = np.unique(x, return_index=True)
-        self._set_order(x if len(u) == len(x) else u[np.argsort(first)])
+        self._set_order(x)
 
     def copy(self):
         new = SparseState(self.N, self.k, dtype=self.dtype, _capacity=self._cur.cap)
         x, a = self._in_order()
-        new.load(x, a)
+        new._load_in_order(x, a)
         new.gamma = self.gamma
         return new
 
@@ -298,7 +303,7 @@ class SparseState:
         x, a = self._in_order()
         idx = np.empty(self.k, dtype=np.int64)
         nat.check(self._eng.L.bass_lcg_choose(n, self.k, int(seed), nat._host(idx)), "bass_lcg_choose")
-        self.load(x[idx], a[idx])
+        self._load_in_order(x[idx], a[idx])
         gsq = self._norm2()
         gl = float(np.sqrt(gsq))
         self._renorm()

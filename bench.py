@@ -57,6 +57,10 @@ def args_parser():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
+    ap.add_argument("--op", default=None, choices=["gate1", "rot1", "gate2", "rdm"],
+                    help="time one op kind on a seeded random state of K entries instead of the "
+                         "workload (a per-kernel microbenchmark; also the small case for ncu)")
+    ap.add_argument("--dtype", default="complex128", choices=["complex128", "complex64"])
     return ap
 
 
@@ -276,6 +280,7 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
         kernels.append({"kernel": nat.SLOT_NAMES[s], "ms": round(float(ms[s]), 3), "launches": int(cnt[s]),
                         "share": round(float(ms[s] / ms.sum()), 4),
                         "gbs": round(nbytes / (ms[s] * 1e-3) / 1e9, 1) if nbytes else None})
+    phases = select_phases(c, nat)
     tile_slots = [s for s in range(30) if ms[s] > 0]
     dom = max(tile_slots, key=lambda s: ms[s])
     per_launch_bytes = 24 * (int(c["prof_in"][dom]) + int(c["prof_out"][dom])) / cnt[dom]
@@ -307,7 +312,108 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
                                        "longest tile pass, the kernels that move the state's own bytes"},
             "note": "algorithmic bytes = 24 B per entry read + 24 B per entry written; timing from a "
                     "profiled step (CUDA events around each launch on its stream)"}
-    return roof, kernels[:12]
+    kernels = kernels[:12]
+    if phases:
+        kernels.append({"kernel": "k_select_coop phases (us per launch)", **phases})
+    return roof, kernels
+
+
+def run_op(a):
+    """One op kind, repeated on a state of K entries: a seeded random state
+    (40-bit keys, Gaussian amplitudes, so |a|^2 is exponentially distributed
+    as in a scrambled circuit).  gate1 / gate2: a Haar-random gate with the
+    simulate-level top-K truncation fused (the state stays at K entries);
+    rot1: a basis-rotation step (rotate, keep the top K, accept if PR drops);
+    rdm: the 1-qubit RDMs of all qubits.  Targets cycle over the qubits.
+    Prints one JSON line: ms per op and the per-kernel table (CUDA events
+    around each launch)."""
+    import numpy as np
+    import torch
+    import ctypes
+    pkg = load_pkg()
+    from bass_b200 import _native as nat
+    from bass_b200.state import SparseState
+    nat.build()
+    L = nat.lib()
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(a.seed)
+    n, K = a.n, a.k
+    x = np.unique(rng.integers(0, 2 ** n, size=K + K // 8 + 64, dtype=np.uint64))[:K]
+    amp = rng.standard_normal(len(x)) + 1j * rng.standard_normal(len(x))
+    amp /= np.sqrt(np.vdot(amp, amp).real)
+    dt = np.dtype(a.dtype)
+    st = SparseState(n, K, dtype=dt, _capacity=K + 16)
+    st.load(x, amp.astype(dt))
+    eng = st._eng
+    tr = nat.trunc(K, K, 1, 1, 1, 0)
+    eng.set_ctrl("pr_cur", 1e300)
+
+    def haar(d):
+        z = (rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))) / np.sqrt(2)
+        qm, r = np.linalg.qr(z)
+        return qm * (np.diag(r) / np.abs(np.diag(r)))
+
+    def one(i):
+        q = (7 * i) % n
+        if a.op == "gate1":
+            st._apply_1q(haar(2), q, tr)
+        elif a.op == "gate2":
+            q2 = (q + 1) % n
+            st._apply_2q(haar(4), q, q2, tr)
+        elif a.op == "rot1":
+            th = 0.3 + 0.1 * (i % 5)
+            U = np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]], dtype=np.complex128)
+            nat.check(L.bass_rotate_step(st._cur.ptr, st._tmp.ptr, nat._host(nat.host_c128(U)), q, K, 0,
+                                         eng.ctrl_ptr, eng.ws_ptr, eng.ws_bytes, eng.stream), "bass_rotate_step")
+            eng.set_ctrl("pr_cur", 1e300)   # every candidate is accepted: the state keeps changing
+        else:
+            nat.check(L.bass_rdm_1q(st._cur.ptr, n, ctypes.c_void_p(nat._ptr(eng.rho)), eng.ctrl_ptr,
+                                    eng.ws_ptr, eng.ws_bytes, eng.stream), "bass_rdm_1q")
+
+    for i in range(a.warmup):
+        one(i)
+    torch.cuda.synchronize()
+    L.bass_profile_enable(1)
+    ms = np.zeros(nat.PROF_SLOTS)
+    cnt = np.zeros(nat.PROF_SLOTS, dtype=np.int64)
+    L.bass_profile_collect(nat._host(ms), nat._host(cnt), nat.PROF_SLOTS)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(a.steps):
+        one(a.warmup + i)
+    e1.record()
+    torch.cuda.synchronize()
+    L.bass_profile_collect(nat._host(ms), nat._host(cnt), nat.PROF_SLOTS)
+    L.bass_profile_enable(0)
+    eng.raise_on_error()
+    c = eng.read_ctrl()
+    kern = []
+    B = 24 if dt == np.complex128 else 16
+    for sl in np.argsort(-ms):
+        if ms[sl] <= 0:
+            break
+        nb = B * (int(c["prof_in"][sl]) + int(c["prof_out"][sl]))
+        kern.append({"kernel": nat.SLOT_NAMES[sl], "us_per_launch": round(1e3 * ms[sl] / max(cnt[sl], 1), 2),
+                     "launches": int(cnt[sl]), "share": round(float(ms[sl] / ms.sum()), 4),
+                     "gbs": round(nb / (ms[sl] * 1e-3) / 1e9, 1) if nb else None})
+    phases = select_phases(c, nat)
+    print(json.dumps({"op": a.op, "K": K, "n_qubits": n, "dtype": a.dtype, "nnz": st.nnz,
+                      "select_phases_us": phases,
+                      "us_per_op": round(1e3 * e0.elapsed_time(e1) / a.steps, 2),
+                      "us_per_op_profiled": round(1e3 * ms.sum() / a.steps, 2), "kernels": kern}), flush=True)
+
+
+def select_phases(c, nat):
+    """Mean microseconds per selection launch of each of its phases."""
+    out = {}
+    for sl in nat.SELECT_PHASE_SLOTS:
+        nl = int(c["prof_out"][sl])
+        if nl:
+            out[nat.SLOT_NAMES[sl]] = round(int(c["prof_in"][sl]) / nl / 1e3, 2)
+    nl = int(c["prof_out"][nat.SELECT_SPEC_SLOT])
+    if nl:
+        out["two_level_frac"] = round(int(c["prof_in"][nat.SELECT_SPEC_SLOT]) / nl, 3)
+    return out
 
 
 def over_ranks(dist, dev, seconds, units):
@@ -330,6 +436,9 @@ def main():
     dist = None
     if a.impl == "reference":
         run_reference(a, rank, world)
+        return
+    if a.op is not None:
+        run_op(a)
         return
     if world > 1:
         import datetime
