@@ -104,10 +104,23 @@ class StatePool:
         self.Uarr = np.zeros((S, 64, 2, 2), np.complex128)
         self.ident = np.ones((S, 64), bool)
         self.stats = {"stages": 0, "launch_calls": 0, "opt_calls": 0, "rotations": 0, "accepted": 0}
+        self.phase0 = 0
 
     # ---- slots -------------------------------------------------------------------------
     def free_slots(self):
         return int((~self.busy).sum())
+
+    def in_phase(self):
+        """Whether a circuit added now reaches its optimisation points (after
+        every optimize_every gates of its own) on the same stages as the
+        circuits already running: then the rotation steps of all of them go
+        to the GPU in the same segmented launches.  True on every
+        optimize_every-th stage since the pool last became non-empty, and
+        whenever it is empty."""
+        if self.optimize_every <= 0 or not self.busy.any():
+            self.phase0 = self.stats["stages"]
+            return True
+        return (self.stats["stages"] - self.phase0) % self.optimize_every == 0
 
     def live(self):
         """Slots with gates left."""
@@ -396,7 +409,7 @@ class BatchedBASS:
         todo = list(range(len(circuits)))[::-1]
         slot_of = {}
         while todo or len(pool.live()) or pool.busy.any():
-            while todo and pool.free_slots():
+            while todo and pool.free_slots() and pool.in_phase():
                 i = todo.pop()
                 slot_of[pool.add(circuits[i], *self.specs[i])] = i
             for c in np.nonzero(pool.busy & (pool.pos >= pool.length))[0]:

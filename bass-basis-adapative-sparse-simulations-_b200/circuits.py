@@ -90,22 +90,66 @@ def config4_batch(seed=0, count=256, n_range=(16, 48), layer_range=(10, 60), h_r
     return specs, circuits
 
 
-def config5_requests(seed=0, count=100, tfim=None, brick_n=(20, 44), brick_depth=(10, 30), brick_m=(12, 22)):
-    """The served workload: ``count`` requests (circuit, n, K), each drawn with
+class Config5Stream:
+    """The served workload as a lazily built sequence of requests (circuit, n,
+    K).  Request i is drawn from its own seeded generator (seed, i): with
     probability 1/2 from the batched workload's TFIM distribution
-    (``config4_batch`` arguments in ``tfim``) or as a brickwork circuit with n,
-    depth and K = 2^m uniform in the given ranges; one seeded generator."""
-    rng = np.random.default_rng(seed)
-    tfim = dict(tfim or {})
-    out = []
-    for _ in range(count):
+    (``config4_batch`` arguments in ``tfim``), otherwise a brickwork circuit
+    with n, depth and K = 2^m uniform in the given ranges.  ``spec(i)`` gives
+    (n, K) without building the circuit; circuits are built on first access."""
+
+    def __init__(self, seed=0, count=100, tfim=None, brick_n=(20, 44), brick_depth=(10, 30), brick_m=(12, 22)):
+        self.seed = int(seed)
+        self.count = int(count)
+        self.tfim = dict(tfim or {})
+        self.brick = (brick_n, brick_depth, brick_m)
+        self._cache = {}
+
+    def __len__(self):
+        return self.count
+
+    def _draw(self, i):
+        rng = np.random.default_rng([self.seed, int(i)])
         if rng.random() < 0.5:
-            sub = int(rng.integers(0, 2 ** 31))
-            (spec,), (circ,) = config4_batch(seed=sub, count=1, **tfim)
-            out.append((circ, spec[0], spec[1]))
-        else:
-            n = int(rng.integers(brick_n[0], brick_n[1] + 1))
-            depth = int(rng.integers(brick_depth[0], brick_depth[1] + 1))
-            m = int(rng.integers(brick_m[0], brick_m[1] + 1))
-            out.append((brickwork_circuit(n, depth, rng=rng), n, 2 ** m))
-    return out
+            t = self.tfim
+            n_range, layer_range = t.get("n_range", (16, 48)), t.get("layer_range", (10, 60))
+            h_range, m_range = t.get("h_range", (0.3, 2.0)), t.get("m_range", (10, 20))
+            n = int(rng.integers(n_range[0], n_range[1] + 1))
+            layers = int(rng.integers(layer_range[0], layer_range[1] + 1))
+            h = float(rng.uniform(h_range[0], h_range[1]))
+            m = int(rng.integers(m_range[0], m_range[1] + 1))
+            return rng, ("tfim", n, layers, h, m)
+        brick_n, brick_depth, brick_m = self.brick
+        n = int(rng.integers(brick_n[0], brick_n[1] + 1))
+        depth = int(rng.integers(brick_depth[0], brick_depth[1] + 1))
+        m = int(rng.integers(brick_m[0], brick_m[1] + 1))
+        return rng, ("brick", n, depth, 0.0, m)
+
+    def spec(self, i):
+        _, (_, n, _, _, m) = self._draw(i)
+        return n, 2 ** m
+
+    def __getitem__(self, i):
+        if i < 0 or i >= self.count:
+            raise IndexError(i)
+        if i not in self._cache:
+            rng, (kind, n, d, h, m) = self._draw(i)
+            if kind == "tfim":
+                t = self.tfim
+                circ = tfim_circuit(n, d, J=1.0, h=h, dt=t.get("dt", 0.05), rng=rng,
+                                    disorder_strength_h=t.get("disorder_h", 0.0))
+            else:
+                circ = brickwork_circuit(n, d, rng=rng)
+            self._cache[i] = (circ, n, 2 ** m)
+        return self._cache[i]
+
+    def release(self, i):
+        """Drop request i's circuit from the cache (after it was served)."""
+        self._cache.pop(i, None)
+
+
+def config5_requests(seed=0, count=100, tfim=None, brick_n=(20, 44), brick_depth=(10, 30), brick_m=(12, 22)):
+    """The served workload: ``count`` requests (circuit, n, K), built at once
+    (see ``Config5Stream`` for the distribution and a lazy form)."""
+    st = Config5Stream(seed, count, tfim, brick_n, brick_depth, brick_m)
+    return [st[i] for i in range(count)]

@@ -57,17 +57,24 @@ class BassServer:
         return state_bytes(num_qubits, k, self.dtype)
 
     def serve(self, requests, arrivals, stop_after=None, clock=time.perf_counter):
-        """requests[i] = (circuit, num_qubits, k).  Runs until every request has
+        """requests[i] = (circuit, num_qubits, k); a sequence with a
+        ``spec(i)`` method giving (num_qubits, k) is read lazily (a request's
+        circuit is fetched when it is admitted).  Runs until every request has
         finished, or until ``stop_after`` seconds (requests still queued or
         running then are abandoned and listed in ``self.unfinished``).
         Returns the finished requests' Results in completion order."""
         import torch
-        n = len(requests)
         order = np.argsort(np.asarray(arrivals, dtype=np.float64), kind="stable")
         arrivals = np.asarray(arrivals, dtype=np.float64)
-        fps = [self.footprint(r[1], r[2]) for r in requests]
-        if any(f > self.budget for f in fps):
-            raise ValueError("a request does not fit the state budget on its own")
+        spec = requests.spec if hasattr(requests, "spec") else (lambda i: tuple(requests[i][1:3]))
+        fps = {}
+
+        def fp(i):
+            if i not in fps:
+                fps[i] = self.footprint(*spec(i))
+                if fps[i] > self.budget:
+                    raise ValueError(f"request {i} does not fit the state budget on its own")
+            return fps[i]
         pool = self.pool = StatePool(max_slots=min(self.max_live, MAX_SEG), dtype=self.dtype, **self.bass_kw)
         incoming = deque(int(i) for i in order)
         waiting = deque()
@@ -83,12 +90,14 @@ class BassServer:
                 break
             while incoming and arrivals[incoming[0]] <= now:
                 waiting.append(incoming.popleft())
-            # admission: FIFO while the footprint fits and a slot is free
-            while waiting and pool.free_slots() and used + fps[waiting[0]] <= self.budget:
+            # admission: FIFO while the footprint fits and a slot is free, on
+            # stages that keep every resident request's optimisation points
+            # on the same stages (their rotation steps then share launches)
+            while waiting and pool.free_slots() and pool.in_phase() and used + fp(waiting[0]) <= self.budget:
                 i = waiting.popleft()
                 c = pool.add(*requests[i])
                 meta[c] = (i, now)
-                used += fps[i]
+                used += fp(i)
             self.peak_bytes = max(self.peak_bytes, used)
             if not pool.busy.any():
                 if incoming:   # idle until the next arrival
@@ -105,8 +114,10 @@ class BassServer:
                 torch.cuda.current_stream().synchronize()
                 r.finish = clock() - t0
                 r.arrival = float(arrivals[r.index])
-                used -= fps[r.index]
+                used -= fp(r.index)
                 done.append(r)
+                if hasattr(requests, "release"):
+                    requests.release(r.index)
         self.elapsed = clock() - t0
         self.unfinished = [i for i, _ in meta.values()] + list(waiting) + list(incoming)
         self.stats = dict(pool.stats)

@@ -61,6 +61,16 @@ def args_parser():
                     help="time one op kind on a seeded random state of K entries instead of the "
                          "workload (a per-kernel microbenchmark; also the small case for ncu)")
     ap.add_argument("--dtype", default="complex128", choices=["complex128", "complex64"])
+    ap.add_argument("--form", default=None, choices=["precision", "batched", "served"],
+                    help="measure one of the other forms instead of the plain workload: precision "
+                         "(complex64 TFIM n=24 K=2^16 against complex128), batched (256 TFIM circuits "
+                         "of uneven size in segmented launches, against the plain path), served "
+                         "(Poisson request stream through BassServer)")
+    ap.add_argument("--count", type=int, default=256, help="batched form: circuits")
+    ap.add_argument("--plain-every", type=int, default=8,
+                    help="batched form: the plain path is timed on every this-many-th circuit")
+    ap.add_argument("--rates", default="50,200,800", help="served form: arrival rates (circuits/s)")
+    ap.add_argument("--seconds", type=float, default=60.0, help="served form: arrival window per rate")
     return ap
 
 
@@ -403,6 +413,175 @@ def run_op(a):
                       "us_per_op_profiled": round(1e3 * ms.sum() / a.steps, 2), "kernels": kern}), flush=True)
 
 
+def overlap_fidelity(x1, a1, x2, a2):
+    """|<1|2>|^2 / (<1|1><2|2>) of two sparse states given as key / amplitude arrays."""
+    import numpy as np
+    a1 = np.asarray(a1, dtype=np.complex128)
+    a2 = np.asarray(a2, dtype=np.complex128)
+    o1 = np.argsort(x1)
+    xs, as1 = np.asarray(x1)[o1], a1[o1]
+    pos = np.searchsorted(xs, x2)
+    pos = np.minimum(pos, max(len(xs) - 1, 0))
+    hit = (len(xs) > 0) & (xs[pos] == x2) if len(xs) else np.zeros(len(x2), bool)
+    ov = np.sum(np.conj(as1[pos[hit]]) * a2[hit]) if len(xs) else 0.0
+    n1 = np.vdot(a1, a1).real
+    n2 = np.vdot(a2, a2).real
+    return float(abs(ov) ** 2 / (n1 * n2)) if n1 > 0 and n2 > 0 else 0.0
+
+
+def timed(fn):
+    """fn() timed with CUDA events on the current stream (synchronised)."""
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1) / 1e3
+
+
+def form_precision(a, pkg):
+    """Config 3: the config-1 TFIM circuit (n=24, 20 layers, K=2^16) with
+    complex64 amplitudes against the complex128 run: throughput of both,
+    fidelity, and the discarded weight of every simulate-level truncation."""
+    import numpy as np
+    from bass_b200.bass import BASS
+    circ = pkg.circuits.config1_circuit(seed=a.seed)
+    n, K = 24, 2 ** 16
+    res = {}
+    for name, dt in [("complex128", np.complex128), ("complex64", np.complex64)]:
+        for _ in range(a.warmup):
+            BASS(n, K, dtype=dt).simulate(circ)
+        ts, ups = [], []
+        for _ in range(a.steps):
+            b = BASS(n, K, dtype=dt)
+            st, t = timed(lambda: b.simulate(circ))
+            ts.append(t)
+            ups.append(b.stats["amp_updates"])
+        rec = BASS(n, K, dtype=dt, record_truncations=True)
+        rst = rec.simulate(circ)
+        res[name] = {"amp_updates_per_s": sum(ups) / sum(ts), "ms_per_circuit": 1e3 * sum(ts) / len(ts),
+                     "state": (rst.x, rst.alpha, rst.gamma, [np.array(u) for u in rec.U]),
+                     "trunc": rec.truncations, "accepted": rec.stats["accepted"]}
+    x1, a1, g1, U1 = res["complex128"]["state"]
+    x2, a2, g2, U2 = res["complex64"]["state"]
+    same_frames = all(np.array_equal(u, v) for u, v in zip(U1, U2))
+    d128 = {i: 1.0 - kept / tot for i, kept, tot in res["complex128"]["trunc"]}
+    d64 = {i: 1.0 - kept / tot for i, kept, tot in res["complex64"]["trunc"]}
+    gates_per_layer = len(circ) // 20
+    per_layer = {}
+    for i in sorted(set(d128) | set(d64)):
+        L = i // gates_per_layer
+        per_layer.setdefault(L, [0.0, 0.0])
+        per_layer[L][0] += d128.get(i, 0.0)
+        per_layer[L][1] += d64.get(i, 0.0)
+    out = {"form": "precision", "workload": "TFIM n=24 20 layers dt=0.1 h~U[0.5,1.5] K=2^16 (config 3)",
+           "complex128": {k: v for k, v in res["complex128"].items() if k in ("amp_updates_per_s", "ms_per_circuit")},
+           "complex64": {k: v for k, v in res["complex64"].items() if k in ("amp_updates_per_s", "ms_per_circuit")},
+           "speedup_c64": res["complex64"]["amp_updates_per_s"] / res["complex128"]["amp_updates_per_s"],
+           "fidelity_c64_vs_c128": overlap_fidelity(x1, a1, x2, a2) if same_frames else None,
+           "same_frames": same_frames, "gamma_sq": {"complex128": g1 ** 2, "complex64": g2 ** 2},
+           "discarded_weight_per_layer": {str(L): {"complex128": v[0], "complex64": v[1]}
+                                          for L, v in sorted(per_layer.items())},
+           "max_layer_discarded_diff": max((abs(v[0] - v[1]) for v in per_layer.values()), default=0.0)}
+    return out
+
+
+def form_batched(a, pkg):
+    """Config 4: ``count`` TFIM circuits of uneven n, depth and K through
+    BatchedBASS (complex64, segmented launches) against the plain complex128
+    path (BASS.simulate one circuit at a time), timed on every
+    ``plain_every``-th circuit; fidelity of the batched result to the plain
+    one on those circuits."""
+    import numpy as np
+    from bass_b200.bass import BASS
+    from bass_b200.batch import BatchedBASS
+    specs, circs = pkg.circuits.config4_batch(seed=a.seed, count=a.count)
+    BatchedBASS(specs[:4], dtype=np.complex64).simulate(circs[:4])   # warm-up: kernels loaded, pools built
+    bb = BatchedBASS(specs, dtype=np.complex64)
+    got, t_batch = timed(lambda: bb.simulate(circs))
+    sample = list(range(0, len(specs), max(1, a.plain_every)))
+    BASS(*specs[sample[0]]).simulate(circs[sample[0]])
+    t_plain, fids, ups_plain = 0.0, [], 0
+    for i in sample:
+        b = BASS(*specs[i])
+        st, t = timed(lambda: b.simulate(circs[i]))
+        t_plain += t
+        ups_plain += b.stats["amp_updates"]
+        fids.append(overlap_fidelity(st.x, st.alpha, got[i].x, got[i].alpha) if not b.stats["accepted"] else None)
+    comparable = [f for f in fids if f is not None]
+    plain_cps = len(sample) / t_plain
+    batch_cps = len(specs) / t_batch
+    # precision on tie-free inputs: the same distribution with site-disordered
+    # fields (a uniform field on the open chain makes mirror-image amplitudes
+    # exactly equal, and complex64 rounding then breaks top-k ties differently)
+    nd = min(64, len(specs))
+    specs_d, circs_d = pkg.circuits.config4_batch(seed=a.seed + 1, count=nd, disorder_h=0.25)
+    got_d = BatchedBASS(specs_d, dtype=np.complex64).simulate(circs_d)
+    fd = []
+    for i in range(nd):
+        b = BASS(*specs_d[i])
+        st = b.simulate(circs_d[i])
+        if not b.stats["accepted"]:
+            fd.append(overlap_fidelity(st.x, st.alpha, got_d[i].x, got_d[i].alpha))
+    return {"form": "batched", "workload": f"{len(specs)} TFIM circuits, n~U[16,48], layers~U[10,60], "
+                                           "h~U[0.3,2], dt=0.05, K=2^U[10,20] (config 4)",
+            "batched_complex64": {"circuits_per_s": batch_cps, "seconds": t_batch,
+                                  "amp_updates_per_s": bb.stats["amp_updates"] / t_batch},
+            "plain_complex128": {"circuits_per_s": plain_cps, "circuits_timed": len(sample), "seconds": t_plain,
+                                 "amp_updates_per_s": ups_plain / t_plain},
+            "speedup_circuits_per_s": batch_cps / plain_cps,
+            "fidelity_min": min(comparable) if comparable else None, "fidelity_compared": len(comparable),
+            "fidelity_below_1e-6": sum(1 for f in comparable if f < 1 - 1e-6),
+            "tie_free": {"circuits": nd, "compared": len(fd), "fidelity_min": min(fd) if fd else None,
+                         "fidelity_below_1e-6": sum(1 for f in fd if f < 1 - 1e-6),
+                         "note": "config-4 distribution with site fields h_i ~ U[h - 0.25, h + 0.25]"},
+            "fidelity_note": "circuits whose plain run accepted a basis rotation are not compared entry by "
+                             "entry (a near-tie PR decision can take another, equally valid trajectory)"}
+
+
+def form_served(a, pkg):
+    """Config 5: open-loop Poisson request streams (one per rate) through
+    BassServer: circuits/s, p50 / p99 latency; the plain path's circuits/s on
+    the same request mix for comparison (every plain_every-th request)."""
+    import numpy as np
+    from bass_b200.bass import BASS
+    from bass_b200.served import BassServer, poisson_arrivals
+    out = {"form": "served", "workload": "requests 50/50 TFIM (config 4 distribution) or brickwork n~U[20,44], "
+                                         "depth~U[10,30], K=2^U[12,22]; 150 GB state budget (config 5)",
+           "seconds_per_rate": a.seconds, "rates": {}}
+    for r, rate in enumerate(float(x) for x in a.rates.split(",")):
+        rng = np.random.default_rng(a.seed + 17 * r)
+        arr = poisson_arrivals(rate, a.seconds, rng)
+        reqs = pkg.circuits.Config5Stream(seed=a.seed + r, count=len(arr))
+        srv = BassServer(budget_bytes=150e9)
+        res = srv.serve(reqs, arr, stop_after=a.seconds + 30.0)
+        summ = srv.summary(res)
+        out["rates"][str(int(rate))] = {k: summ[k] for k in ("completed", "unfinished", "circuits_per_s", "p50_s",
+                                                            "p99_s", "elapsed_s", "peak_state_bytes")}
+        out["rates"][str(int(rate))]["offered"] = len(arr)
+    reqs = pkg.circuits.config5_requests(seed=a.seed, count=max(8, 4 * a.plain_every))
+    sample = reqs[::max(1, a.plain_every // 2)]
+    t_plain = 0.0
+    for circ, n, k in sample:
+        b = BASS(n, k)
+        _, t = timed(lambda: b.simulate(circ))
+        t_plain += t
+    out["plain_complex128_circuits_per_s"] = len(sample) / t_plain
+    return out
+
+
+def run_form(a):
+    import torch
+    pkg = load_pkg()
+    from bass_b200 import _native
+    _native.build()
+    torch.cuda.set_device(0)
+    fn = {"precision": form_precision, "batched": form_batched, "served": form_served}[a.form]
+    print(json.dumps(fn(a, pkg)), flush=True)
+
+
 def select_phases(c, nat):
     """Mean microseconds per selection launch of each of its phases."""
     out = {}
@@ -439,6 +618,9 @@ def main():
         return
     if a.op is not None:
         run_op(a)
+        return
+    if a.form is not None:
+        run_form(a)
         return
     if world > 1:
         import datetime
