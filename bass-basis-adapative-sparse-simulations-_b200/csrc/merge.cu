@@ -398,7 +398,9 @@ __device__ void finalize_op(const OpArgs& a, const bass_trunc& tr, int mode, int
   out->rscale[0] = 1.0;
   out->rscale[1] = 1.0;
   if (kind == K_PERM) return;  // first pass of a 2-qubit gate: no bookkeeping
-  c->amp_updates += n_in;
+  // an amplitude update is an input entry of a gate or a rotation step; a
+  // plain truncation (K_IDENT) transforms nothing
+  if (kind != K_IDENT) c->amp_updates += n_in;
   c->n_ops += 1;
   const int trunc = sel->do_trunc;
   if (mode == 1) {

@@ -31,7 +31,8 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "bass-basis-adapative-sparse-simulations-_b200")
-CPU_SAMPLE_GATES = 28
+CPU_SAMPLE_GATES = 26   # the CPU sample: these gates, then a coordinate-descent pass ...
+CPU_SAMPLE_QUBITS = 12  # ... over these first qubits
 
 
 def load_pkg():
@@ -57,9 +58,10 @@ def args_parser():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
-    ap.add_argument("--op", default=None, choices=["gate1", "rot1", "gate2", "rdm"],
-                    help="time one op kind on a seeded random state of K entries instead of the "
-                         "workload (a per-kernel microbenchmark; also the small case for ncu)")
+    ap.add_argument("--op", default=None,
+                    help="comma-separated op kinds (gate1, rot1, gate2, rdm): time each on a seeded random "
+                         "state of K entries instead of the workload (a per-kernel microbenchmark; also "
+                         "the small case for ncu)")
     ap.add_argument("--dtype", default="complex128", choices=["complex128", "complex64"])
     ap.add_argument("--form", default=None, choices=["precision", "batched", "served"],
                     help="measure one of the other forms instead of the plain workload: precision "
@@ -126,15 +128,41 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline (oracle port of the reference's algorithm)
 # ---------------------------------------------------------------------------
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_sample(circuit, n, k):
+    """The CPU oracle (the reference's algorithm restated in C, driven like
+    BASS.simulate) on every host thread: the workload's first CPU_SAMPLE_GATES
+    gates (the state grows to K and truncation starts), then one pass of the
+    basis optimisation over the first CPU_SAMPLE_QUBITS qubits (the RDMs, then
+    for each qubit a rotation step with top-K and the PR decision).  Returns (amp-updates, seconds,
+    rotation steps, threads); updates are counted as on the GPU (one input
+    entry of a gate or rotation step)."""
     sys.path.insert(0, ROOT)
     from oracle import oracle
     oracle.build()
+    threads = oracle.set_threads(0)
     b = oracle.OracleBASS(n, k)
     t0 = time.perf_counter()
-    b.simulate(circuit[:CPU_SAMPLE_GATES])
+    st = b.simulate(circuit[:CPU_SAMPLE_GATES])
+    b._descent_pass(st, range(min(n, CPU_SAMPLE_QUBITS)))
     dt = time.perf_counter() - t0
-    return b.stats["amp_updates"], dt
+    return b.stats["amp_updates"], dt, b.stats["rotations"], threads
+
+
+def cpu_sample_text(k, dt, u, rot, threads):
+    return (f"first {CPU_SAMPLE_GATES} gates of the workload circuit at K={k}, then one basis-optimisation pass "
+            f"over qubits 0-{CPU_SAMPLE_QUBITS - 1} ({rot} rotation steps with top-K, one RDM), {threads} threads on {cpu_model()} "
+            f"({dt:.1f} s, {u} updates)")
 
 
 def run_reference(a, rank, world):
@@ -142,22 +170,22 @@ def run_reference(a, rank, world):
         return
     pkg = load_pkg()
     circ = pkg.circuits.config2_circuit(seed=a.seed, num_qubits=a.n, depth=a.depth)
-    for _ in range(a.warmup):
-        cpu_sample(circ, a.n, a.k)
+    for _ in range(a.warmup):   # loads and warms the oracle (a small budget: seconds, not minutes)
+        cpu_sample(circ, a.n, 2 ** 10)
     ups, secs = [], []
     for _ in range(a.steps):
-        u, dt = cpu_sample(circ, a.n, a.k)
+        u, dt, rot, threads = cpu_sample(circ, a.n, a.k)
         ups.append(u)
         secs.append(dt)
     value = sum(ups) / sum(secs)
-    sample = f"first {CPU_SAMPLE_GATES} gates of the workload circuit at K={a.k}, per step"
+    sample = "per step: " + cpu_sample_text(a.k, sum(secs) / len(secs), ups[0], rot, threads)
     line = {
         "impl": "reference", "metric": "amp_updates_per_s", "value": value, "unit": "amp-updates/s",
         "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
         "data": "synthetic (seeded brickwork circuit)",
         "config": workload_config(a),
-        "cpu_baseline": {"value": value, "unit": "amp-updates/s", "cores": 1, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "amp-updates/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "amp-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -245,10 +273,9 @@ def run_ours(a, rank, world, dist):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        u, dt = cpu_sample(circ, a.n, a.k)
-        cpu = {"value": u / dt, "unit": "amp-updates/s", "cores": 1, "kind": "port",
-               "sample": f"first {CPU_SAMPLE_GATES} gates of the workload circuit at K={a.k} "
-                         f"({dt:.1f} s, {u} updates)"}
+        u, dt, rot, threads = cpu_sample(circ, a.n, a.k)
+        cpu = {"value": u / dt, "unit": "amp-updates/s", "cores": threads, "kind": "port",
+               "sample": cpu_sample_text(a.k, dt, u, rot, threads)}
 
     if rank == 0:
         line = {
@@ -429,6 +456,12 @@ def overlap_fidelity(x1, a1, x2, a2):
     return float(abs(ov) ** 2 / (n1 * n2)) if n1 > 0 and n2 > 0 else 0.0
 
 
+def identity_frames(U):
+    """Every frame of a finished batched / served state is the identity."""
+    import numpy as np
+    return all(np.array_equal(np.asarray(u), np.eye(2)) for u in U)
+
+
 def timed(fn):
     """fn() timed with CUDA events on the current stream (synchronised)."""
     import torch
@@ -509,7 +542,8 @@ def form_batched(a, pkg):
         st, t = timed(lambda: b.simulate(circs[i]))
         t_plain += t
         ups_plain += b.stats["amp_updates"]
-        fids.append(overlap_fidelity(st.x, st.alpha, got[i].x, got[i].alpha) if not b.stats["accepted"] else None)
+        fids.append(overlap_fidelity(st.x, st.alpha, got[i].x, got[i].alpha)
+                    if not b.stats["accepted"] and identity_frames(got[i].U) else None)
     comparable = [f for f in fids if f is not None]
     plain_cps = len(sample) / t_plain
     batch_cps = len(specs) / t_batch
@@ -519,11 +553,13 @@ def form_batched(a, pkg):
     nd = min(64, len(specs))
     specs_d, circs_d = pkg.circuits.config4_batch(seed=a.seed + 1, count=nd, disorder_h=0.25)
     got_d = BatchedBASS(specs_d, dtype=np.complex64).simulate(circs_d)
-    fd = []
+    fd, split = [], 0
     for i in range(nd):
         b = BASS(*specs_d[i])
         st = b.simulate(circs_d[i])
-        if not b.stats["accepted"]:
+        same = not b.stats["accepted"] and identity_frames(got_d[i].U)
+        split += (not b.stats["accepted"]) != identity_frames(got_d[i].U)
+        if same:
             fd.append(overlap_fidelity(st.x, st.alpha, got_d[i].x, got_d[i].alpha))
     return {"form": "batched", "workload": f"{len(specs)} TFIM circuits, n~U[16,48], layers~U[10,60], "
                                            "h~U[0.3,2], dt=0.05, K=2^U[10,20] (config 4)",
@@ -536,9 +572,11 @@ def form_batched(a, pkg):
             "fidelity_below_1e-6": sum(1 for f in comparable if f < 1 - 1e-6),
             "tie_free": {"circuits": nd, "compared": len(fd), "fidelity_min": min(fd) if fd else None,
                          "fidelity_below_1e-6": sum(1 for f in fd if f < 1 - 1e-6),
+                         "rotation_decisions_differ": split,
                          "note": "config-4 distribution with site fields h_i ~ U[h - 0.25, h + 0.25]"},
-            "fidelity_note": "circuits whose plain run accepted a basis rotation are not compared entry by "
-                             "entry (a near-tie PR decision can take another, equally valid trajectory)"}
+            "fidelity_note": "compared entry by entry where neither run kept a basis rotation (both in the "
+                             "computational basis); a run that kept one holds its state in another frame, and "
+                             "a near-tie PR decision can go either way under complex64 rounding"}
 
 
 def form_served(a, pkg):
@@ -617,7 +655,13 @@ def main():
         run_reference(a, rank, world)
         return
     if a.op is not None:
-        run_op(a)
+        import copy
+        for op in a.op.split(","):
+            if op not in ("gate1", "rot1", "gate2", "rdm"):
+                raise SystemExit(f"unknown op {op}")
+            b = copy.copy(a)
+            b.op = op
+            run_op(b)
         return
     if a.form is not None:
         run_form(a)

@@ -136,23 +136,160 @@ static inline void oht_put(oht* h, uint64_t key, int64_t val) {
 }
 
 /* ------------------------------------------------------------------ */
+/* parallel building blocks.  With -fopenmp the heavy kernels below run */
+/* on every host thread; their results do not depend on the thread     */
+/* count (work is split into contiguous ranges, sorts are stable, every */
+/* sum is exact), so they equal the single-threaded ones bit for bit.   */
+/* ------------------------------------------------------------------ */
+#ifdef _OPENMP
+#include <omp.h>
+static int par_tid(void) { return omp_get_thread_num(); }
+static int par_avail(void) { return omp_get_max_threads(); }
+#else
+static int par_tid(void) { return 0; }
+static int par_avail(void) { return 1; }
+#endif
+static int g_threads = 1;  /* threads the kernels may use (orc_set_threads) */
+static int par_max(void) { return g_threads; }
+
+/* threads for n items: at most one per 32768 items */
+static int par_threads_for(int64_t n) {
+  int t = par_max();
+  if ((int64_t)t > n / 32768) t = (int)(n / 32768);
+  return t < 1 ? 1 : t;
+}
+/* start of range t of T contiguous ranges over [0, n) */
+static inline int64_t par_lo(int64_t n, int T, int t) { return (int64_t)(((i128)n * t) / T); }
+
+/* Threads the kernels may use: n > 0 that many (at most the OpenMP maximum),
+   n <= 0 every host thread OpenMP offers.  The default is one.  Returns the
+   number set. */
+int orc_set_threads(int n) {
+  const int avail = par_avail();
+  g_threads = (n <= 0 || n > avail) ? avail : n;
+  return g_threads;
+}
+int orc_threads(void) { return par_max(); }
+
+/* Stable LSD radix sort of keys[0..n) carrying a payload of psize (8 or 16)
+   bytes per item, 11-bit digits; a digit that is the same for every item is
+   skipped (a stable pass over it changes nothing).  Items are spread over
+   threads in contiguous ranges and placed by (digit, thread) offsets, so the
+   order is that of a sequential stable sort. */
+static int par_radix_sort(uint64_t* keys, void* pay, size_t psize, int64_t n) {
+  if (n <= 1) return 0;
+  enum { RB = 11, NB = 1 << RB };
+  const int T = par_threads_for(n);
+  uint64_t* tk = (uint64_t*)malloc((size_t)n * sizeof(uint64_t));
+  char* tp = (char*)malloc((size_t)n * psize);
+  int64_t* cnt = (int64_t*)malloc((size_t)T * NB * sizeof(int64_t));
+  if (!tk || !tp || !cnt) { free(tk); free(tp); free(cnt); return -1; }
+  uint64_t *ks = keys, *kd = tk;
+  char *ps = (char*)pay, *pd = tp;
+  for (int shift = 0; shift < 64; shift += RB) {
+    memset(cnt, 0, (size_t)T * NB * sizeof(int64_t));
+#pragma omp parallel num_threads(T)
+    {
+      const int t = par_tid();
+      int64_t* c = cnt + (size_t)t * NB;
+      for (int64_t i = par_lo(n, T, t); i < par_lo(n, T, t + 1); ++i) c[(ks[i] >> shift) & (NB - 1)]++;
+    }
+    int single = 0;
+    for (int d = 0; d < NB && !single; ++d) {
+      int64_t tot = 0;
+      for (int t = 0; t < T; ++t) tot += cnt[(size_t)t * NB + d];
+      if (tot == n) single = 1;
+    }
+    if (single) continue;
+    int64_t run = 0;
+    for (int d = 0; d < NB; ++d)
+      for (int t = 0; t < T; ++t) {
+        const int64_t c = cnt[(size_t)t * NB + d];
+        cnt[(size_t)t * NB + d] = run;
+        run += c;
+      }
+#pragma omp parallel num_threads(T)
+    {
+      const int t = par_tid();
+      int64_t* c = cnt + (size_t)t * NB;
+      for (int64_t i = par_lo(n, T, t); i < par_lo(n, T, t + 1); ++i) {
+        const int64_t d = c[(ks[i] >> shift) & (NB - 1)]++;
+        kd[d] = ks[i];
+        if (psize == 16) memcpy(pd + (size_t)d * 16, ps + (size_t)i * 16, 16);
+        else memcpy(pd + (size_t)d * 8, ps + (size_t)i * 8, 8);
+      }
+    }
+    uint64_t* tku = ks; ks = kd; kd = tku;
+    char* tpc = ps; ps = pd; pd = tpc;
+  }
+  if (ks != keys) {
+    memcpy(keys, ks, (size_t)n * sizeof(uint64_t));
+    memcpy(pay, ps, (size_t)n * psize);
+  }
+  free(tk); free(tp); free(cnt);
+  return 0;
+}
+
+/* exact sum of |a|^2 (sq = 0) or |a|^4 (sq = 1) over a[0..n) */
+static i128 par_sum_p(const cd* a, int64_t n, int sq) {
+  const int T = par_threads_for(n);
+  i128 part[256];
+  const int TT = T > 256 ? 256 : T;
+#pragma omp parallel num_threads(TT)
+  {
+    const int t = par_tid();
+    i128 s = 0;
+    for (int64_t i = par_lo(n, TT, t); i < par_lo(n, TT, t + 1); ++i) {
+      const double p = cd_p(a[i]);
+      s += fx_from(sq ? p * p : p);
+    }
+    part[t] = s;
+  }
+  i128 s = 0;
+  for (int t = 0; t < TT; ++t) s += part[t];
+  return s;
+}
+
+/* ------------------------------------------------------------------ */
 /* sparse_state.py:15-67  apply_1qubit_gate_kernel_opt                */
 /* ------------------------------------------------------------------ */
-int64_t orc_expand_1q(const uint64_t* x_in, const cd* a_in, int64_t nnz_in,
-                      uint64_t* x_out, cd* a_out, const cd* G, int q) {
+static int64_t expand_1q_range(const uint64_t* x_in, const cd* a_in, int64_t lo, int64_t hi,
+                               uint64_t* x_out, cd* a_out, const cd* G, int q, int write) {
   int64_t n = 0;
   uint64_t m = 1ULL << q;
   cd g00 = G[0], g01 = G[1], g10 = G[2], g11 = G[3];
-  for (int64_t i = 0; i < nnz_in; ++i) {
+  for (int64_t i = lo; i < hi; ++i) {
     uint64_t x = x_in[i];
     cd a = a_in[i];
     uint64_t base = x & ~m;
     cd o0, o1;
     if (((x >> q) & 1ULL) == 0) { o0 = cd_mul(g00, a); o1 = cd_mul(g10, a); }
     else { o0 = cd_mul(g01, a); o1 = cd_mul(g11, a); }
-    if (cd_nz(o0)) { x_out[n] = base; a_out[n] = o0; ++n; }
-    if (cd_nz(o1)) { x_out[n] = base | m; a_out[n] = o1; ++n; }
+    if (cd_nz(o0)) { if (write) { x_out[n] = base; a_out[n] = o0; } ++n; }
+    if (cd_nz(o1)) { if (write) { x_out[n] = base | m; a_out[n] = o1; } ++n; }
   }
+  return n;
+}
+int64_t orc_expand_1q(const uint64_t* x_in, const cd* a_in, int64_t nnz_in,
+                      uint64_t* x_out, cd* a_out, const cd* G, int q) {
+  const int T = par_threads_for(nnz_in);
+  if (T == 1) return expand_1q_range(x_in, a_in, 0, nnz_in, x_out, a_out, G, q, 1);
+  int64_t* off = (int64_t*)calloc((size_t)T + 1, sizeof(int64_t));
+  if (!off) return -2;
+#pragma omp parallel num_threads(T)
+  {
+    const int t = par_tid();
+    off[t + 1] = expand_1q_range(x_in, a_in, par_lo(nnz_in, T, t), par_lo(nnz_in, T, t + 1), 0, 0, G, q, 0);
+  }
+  for (int t = 0; t < T; ++t) off[t + 1] += off[t];
+#pragma omp parallel num_threads(T)
+  {
+    const int t = par_tid();
+    expand_1q_range(x_in, a_in, par_lo(nnz_in, T, t), par_lo(nnz_in, T, t + 1), x_out + off[t], a_out + off[t],
+                    G, q, 1);
+  }
+  const int64_t n = off[T];
+  free(off);
   return n;
 }
 
@@ -185,40 +322,52 @@ int64_t orc_expand_2q(const uint64_t* x_in, const cd* a_in, int64_t nnz_in,
    A pass whose digit is constant over the input is a no-op for a stable
    sort, so it is skipped (the result is identical). */
 int orc_radix_sort(uint64_t* keys, cd* vals, int64_t n) {
-  if (n <= 1) return 0;
-  uint64_t* tk = (uint64_t*)malloc((size_t)n * sizeof(uint64_t));
-  cd* tv = (cd*)malloc((size_t)n * sizeof(cd));
-  int64_t* cnt = (int64_t*)malloc(65536 * sizeof(int64_t));
-  if (!tk || !tv || !cnt) { free(tk); free(tv); free(cnt); return -1; }
-  for (int shift = 0; shift < 64; shift += 16) {
-    memset(cnt, 0, 65536 * sizeof(int64_t));
-    for (int64_t i = 0; i < n; ++i) cnt[(keys[i] >> shift) & 0xFFFF]++;
-    int single = 0;
-    for (int b = 0; b < 65536; ++b) if (cnt[b] == n) { single = 1; break; }
-    if (single) continue;
-    int64_t s = 0;
-    for (int b = 0; b < 65536; ++b) { int64_t c = cnt[b]; cnt[b] = s; s += c; }
-    for (int64_t i = 0; i < n; ++i) {
-      int64_t d = cnt[(keys[i] >> shift) & 0xFFFF]++;
-      tk[d] = keys[i]; tv[d] = vals[i];
-    }
-    memcpy(keys, tk, (size_t)n * sizeof(uint64_t));
-    memcpy(vals, tv, (size_t)n * sizeof(cd));
-  }
-  free(tk); free(tv); free(cnt);
-  return 0;
+  return par_radix_sort(keys, vals, sizeof(cd), n);
 }
 
 /* sparse_state.py:127-147  merge_sorted_kernel: sum adjacent equal keys in
    place (left to right); sums that cancel to zero are kept. */
 int64_t orc_merge_sorted(uint64_t* x, cd* a, int64_t nnz) {
   if (nnz == 0) return 0;
-  int64_t w = 0;
-  for (int64_t r = 1; r < nnz; ++r) {
-    if (x[r] == x[w]) a[w] = cd_add(a[w], a[r]);
-    else { ++w; x[w] = x[r]; a[w] = a[r]; }
+  const int T = par_threads_for(nnz);
+  if (T == 1) {
+    int64_t w = 0;
+    for (int64_t r = 1; r < nnz; ++r) {
+      if (x[r] == x[w]) a[w] = cd_add(a[w], a[r]);
+      else { ++w; x[w] = x[r]; a[w] = a[r]; }
+    }
+    return w + 1;
   }
-  return w + 1;
+  /* runs of equal keys, each summed left to right by the thread whose range
+     holds the run's first item, written to a copy at the run's rank */
+  int64_t* off = (int64_t*)calloc((size_t)T + 1, sizeof(int64_t));
+  uint64_t* tx = (uint64_t*)malloc((size_t)nnz * sizeof(uint64_t));
+  cd* ta = (cd*)malloc((size_t)nnz * sizeof(cd));
+  if (!off || !tx || !ta) { free(off); free(tx); free(ta); return -2; }
+#pragma omp parallel num_threads(T)
+  {
+    const int t = par_tid();
+    int64_t c = 0;
+    for (int64_t i = par_lo(nnz, T, t); i < par_lo(nnz, T, t + 1); ++i) c += (i == 0 || x[i] != x[i - 1]);
+    off[t + 1] = c;
+  }
+  for (int t = 0; t < T; ++t) off[t + 1] += off[t];
+#pragma omp parallel num_threads(T)
+  {
+    const int t = par_tid();
+    int64_t w = off[t];
+    for (int64_t i = par_lo(nnz, T, t); i < par_lo(nnz, T, t + 1); ++i) {
+      if (!(i == 0 || x[i] != x[i - 1])) continue;
+      cd acc = a[i];
+      for (int64_t r = i + 1; r < nnz && x[r] == x[i]; ++r) acc = cd_add(acc, a[r]);
+      tx[w] = x[i]; ta[w] = acc; ++w;
+    }
+  }
+  const int64_t n = off[T];
+  memcpy(x, tx, (size_t)n * sizeof(uint64_t));
+  memcpy(a, ta, (size_t)n * sizeof(cd));
+  free(off); free(tx); free(ta);
+  return n;
 }
 
 /* SparseState.apply_single_qubit_gate (sparse_state.py:268-296) without the
@@ -301,6 +450,7 @@ int64_t orc_apply_2q_sorted(const uint64_t* x_in, const cd* a_in, int64_t nnz_in
 
 /* sparse_state.py:178-190  apply_2qubit_diagonal_kernel (in place) */
 void orc_phase_2q(const uint64_t* x, cd* a, int64_t nnz, int q1, int q2, const cd* diag) {
+#pragma omp parallel for num_threads(par_threads_for(nnz)) schedule(static)
   for (int64_t i = 0; i < nnz; ++i) {
     int b1 = (int)((x[i] >> q1) & 1ULL), b2 = (int)((x[i] >> q2) & 1ULL);
     a[i] = cd_mul(a[i], diag[(b1 << 1) | b2]);
@@ -310,57 +460,105 @@ void orc_phase_2q(const uint64_t* x, cd* a, int64_t nnz, int q1, int q2, const c
 /* ------------------------------------------------------------------ */
 /* top-k selection by (p descending, key ascending)                    */
 /* ------------------------------------------------------------------ */
-typedef struct { double p; uint64_t k; } pk;
-static inline int pk_before(pk a, pk b) {  /* a ranks strictly above b */
-  return a.p > b.p || (a.p == b.p && a.k < b.k);
-}
-static uint64_t sel_rng = 0x9E3779B97F4A7C15ULL;
-/* returns the element of rank r (0 = best) of v[0..n), reordering v */
-static pk pk_select(pk* v, int64_t n, int64_t r) {
-  int64_t lo = 0, hi = n - 1;
-  while (hi > lo) {
-    sel_rng = sel_rng * 6364136223846793005ULL + 1442695040888963407ULL;
-    int64_t pi = lo + (int64_t)((sel_rng >> 33) % (uint64_t)(hi - lo + 1));
-    pk piv = v[pi];
-    /* three-way partition: [lo,lt) before piv, [lt,gt] equal, (gt,hi] after */
-    int64_t lt = lo, i = lo, gt = hi;
-    while (i <= gt) {
-      if (pk_before(v[i], piv)) { pk t = v[lt]; v[lt] = v[i]; v[i] = t; ++lt; ++i; }
-      else if (pk_before(piv, v[i])) { pk t = v[gt]; v[gt] = v[i]; v[i] = t; --gt; }
-      else ++i;
-    }
-    if (r < lt) hi = lt - 1;
-    else if (r > gt) lo = gt + 1;
-    else return v[r];
-  }
-  return v[lo];
-}
-
 /* Keep the k best entries of (x, a)[0..n) in their input order.  Returns the
-   new count; *kept = sum of kept |a|^2, *total = sum of all |a|^2 (both in
-   array order).  If n <= k nothing is removed. */
+   new count; *kept = sum of kept |a|^2, *total = sum of all |a|^2 (both
+   exact).  If n <= k nothing is removed.  The threshold is the entry of rank
+   k - 1 by (|a|^2 descending, key ascending): found by a radix select on the
+   bit patterns of |a|^2 (non-negative doubles order as their bits), then, for
+   the entries whose |a|^2 equals the threshold, by their keys. */
+static int u64_cmp(const void* A, const void* B) {
+  const uint64_t a = *(const uint64_t*)A, b = *(const uint64_t*)B;
+  return (a > b) - (a < b);
+}
 int64_t orc_select_topk(uint64_t* x, cd* a, int64_t n, int64_t k, double* kept, double* total) {
-  i128 acc = 0;
-  for (int64_t i = 0; i < n; ++i) acc += fx_from(cd_p(a[i]));
-  double tot = fx_to(acc);
+  const double tot = fx_to(par_sum_p(a, n, 0));
   if (total) *total = tot;
   if (n <= k) { if (kept) *kept = tot; return n; }
   if (k <= 0) { if (kept) *kept = 0.0; return 0; }
-  pk* v = (pk*)malloc((size_t)n * sizeof(pk));
-  if (!v) return -2;
-  for (int64_t i = 0; i < n; ++i) { v[i].p = cd_p(a[i]); v[i].k = x[i]; }
-  pk th = pk_select(v, n, k - 1);
-  free(v);
-  int64_t w = 0;
-  i128 kacc = 0;
+  const int T = par_threads_for(n);
+  enum { RB = 11, NB = 1 << RB };
+  uint64_t* pb = (uint64_t*)malloc((size_t)n * sizeof(uint64_t));
+  int64_t* cnt = (int64_t*)malloc((size_t)T * NB * sizeof(int64_t));
+  if (!pb || !cnt) { free(pb); free(cnt); return -2; }
+#pragma omp parallel for num_threads(T) schedule(static)
   for (int64_t i = 0; i < n; ++i) {
-    pk e; e.p = cd_p(a[i]); e.k = x[i];
-    if (!pk_before(th, e)) {  /* e ranks at or above the threshold */
-      kacc += fx_from(e.p);
-      x[w] = x[i]; a[w] = a[i]; ++w;
-    }
+    const double p = cd_p(a[i]);
+    memcpy(&pb[i], &p, sizeof p);
   }
+  /* digits from the top: bits [53, 64), [42, 53), ..., [9, 20), [0, 9) */
+  uint64_t pre = 0;   /* the fixed high bits of the threshold pattern */
+  int64_t need = k;   /* rank, among the entries matching pre, still to place */
+  int fixed = 64;     /* bits >= fixed are fixed in pre */
+  while (fixed > 0) {
+    const int shift = fixed >= RB ? fixed - RB : 0;
+    const int width = fixed - shift;
+    const uint64_t dmask = (1ULL << width) - 1;
+    memset(cnt, 0, (size_t)T * NB * sizeof(int64_t));
+#pragma omp parallel num_threads(T)
+    {
+      const int t = par_tid();
+      int64_t* c = cnt + (size_t)t * NB;
+      for (int64_t i = par_lo(n, T, t); i < par_lo(n, T, t + 1); ++i)
+        if (fixed == 64 || (pb[i] >> fixed) == (pre >> fixed)) c[(pb[i] >> shift) & dmask]++;
+    }
+    int64_t above = 0;
+    int d = (int)dmask;
+    for (; d > 0; --d) {
+      int64_t c = 0;
+      for (int t = 0; t < T; ++t) c += cnt[(size_t)t * NB + d];
+      if (above + c >= need) break;
+      above += c;
+    }
+    need -= above;
+    pre |= (uint64_t)d << shift;
+    fixed = shift;
+  }
+  /* the entries at the threshold pattern: the need-th smallest key */
+  int64_t m = 0;
+  for (int64_t i = 0; i < n; ++i) m += (pb[i] == pre);
+  uint64_t* tk = (uint64_t*)malloc((size_t)(m > 0 ? m : 1) * sizeof(uint64_t));
+  if (!tk) { free(pb); free(cnt); return -2; }
+  m = 0;
+  for (int64_t i = 0; i < n; ++i) if (pb[i] == pre) tk[m++] = x[i];
+  qsort(tk, (size_t)m, sizeof(uint64_t), u64_cmp);
+  const uint64_t key_t = tk[need - 1];
+  free(tk);
+  /* the survivors, in input order: counts per range, then the copies */
+  int64_t* off = (int64_t*)calloc((size_t)T + 1, sizeof(int64_t));
+  i128* ks = (i128*)calloc((size_t)T, sizeof(i128));
+  uint64_t* tx = (uint64_t*)malloc((size_t)n * sizeof(uint64_t));
+  cd* ta = (cd*)malloc((size_t)n * sizeof(cd));
+  if (!off || !ks || !tx || !ta) { free(off); free(ks); free(tx); free(ta); free(pb); free(cnt); return -2; }
+#pragma omp parallel num_threads(T)
+  {
+    const int t = par_tid();
+    int64_t c = 0;
+    for (int64_t i = par_lo(n, T, t); i < par_lo(n, T, t + 1); ++i)
+      c += pb[i] > pre || (pb[i] == pre && x[i] <= key_t);
+    off[t + 1] = c;
+  }
+  for (int t = 0; t < T; ++t) off[t + 1] += off[t];
+#pragma omp parallel num_threads(T)
+  {
+    const int t = par_tid();
+    int64_t w = off[t];
+    i128 acc = 0;
+    for (int64_t i = par_lo(n, T, t); i < par_lo(n, T, t + 1); ++i) {
+      if (!(pb[i] > pre || (pb[i] == pre && x[i] <= key_t))) continue;
+      double p;
+      memcpy(&p, &pb[i], sizeof p);
+      acc += fx_from(p);
+      tx[w] = x[i]; ta[w] = a[i]; ++w;
+    }
+    ks[t] = acc;
+  }
+  const int64_t w = off[T];
+  i128 kacc = 0;
+  for (int t = 0; t < T; ++t) kacc += ks[t];
+  memcpy(x, tx, (size_t)w * sizeof(uint64_t));
+  memcpy(a, ta, (size_t)w * sizeof(cd));
   if (kept) *kept = fx_to(kacc);
+  free(off); free(ks); free(tx); free(ta); free(pb); free(cnt);
   return w;
 }
 
@@ -417,25 +615,36 @@ int orc_rdm_all(const uint64_t* x, const cd* a, int64_t nnz, int N, cd* rho) {
   oht h;
   if (!acc || oht_init(&h, nnz)) { free(acc); return -2; }
   for (int64_t i = 0; i < nnz; ++i) oht_put(&h, x[i], i);
-  for (int64_t i = 0; i < nnz; ++i) {
-    uint64_t xi = x[i];
-    cd ai = a[i];
-    i128 prob = fx_from(ai.re * ai.re + ai.im * ai.im);
-    for (int q = 0; q < N; ++q) {
-      int bit = (int)((xi >> q) & 1ULL);
-      i128* r = acc + (size_t)q * 4;
-      r[bit] += prob;
-      if (bit == 0) {
-        int64_t p = oht_find(&h, xi | (1ULL << q));
-        if (p >= 0) {
-          cd caj = {a[p].re, -a[p].im};
-          cd t = cd_mul(ai, caj);
-          r[2] += fx_from(t.re);
-          r[3] += fx_from(t.im);
+  const int T = par_threads_for(nnz);
+  i128* tacc = (i128*)calloc((size_t)T * N * 4, sizeof(i128));
+  if (!tacc) { oht_free(&h); free(acc); return -2; }
+#pragma omp parallel num_threads(T)
+  {
+    const int th = par_tid();
+    i128* my = tacc + (size_t)th * N * 4;
+    for (int64_t i = par_lo(nnz, T, th); i < par_lo(nnz, T, th + 1); ++i) {
+      uint64_t xi = x[i];
+      cd ai = a[i];
+      i128 prob = fx_from(ai.re * ai.re + ai.im * ai.im);
+      for (int q = 0; q < N; ++q) {
+        int bit = (int)((xi >> q) & 1ULL);
+        i128* r = my + (size_t)q * 4;
+        r[bit] += prob;
+        if (bit == 0) {
+          int64_t p = oht_find(&h, xi | (1ULL << q));
+          if (p >= 0) {
+            cd caj = {a[p].re, -a[p].im};
+            cd t = cd_mul(ai, caj);
+            r[2] += fx_from(t.re);
+            r[3] += fx_from(t.im);
+          }
         }
       }
     }
   }
+  for (int th = 0; th < T; ++th)
+    for (int v = 0; v < N * 4; ++v) acc[v] += tacc[(size_t)th * N * 4 + v];
+  free(tacc);
   for (int q = 0; q < N; ++q) {
     cd* r = rho + (size_t)q * 4;
     i128* c = acc + (size_t)q * 4;
@@ -482,30 +691,62 @@ static int ri_cmp(const void* A, const void* B) {
   if (a->r > b->r) return 1;
   return (a->i < b->i) ? -1 : (a->i > b->i);
 }
-int64_t orc_rotate_1q(const uint64_t* x, const cd* a, int64_t nnz, int qubit, const cd* U,
-                      uint64_t* x_out, cd* a_out) {
-  uint64_t m = 1ULL << qubit;
-  ri* v = (ri*)malloc((size_t)(nnz > 0 ? nnz : 1) * sizeof(ri));
-  if (!v) return -2;
-  for (int64_t i = 0; i < nnz; ++i) { v[i].r = x[i] & ~m; v[i].i = i; }
-  qsort(v, (size_t)nnz, sizeof(ri), ri_cmp);
-  int64_t n = 0, i = 0;
-  while (i < nnz) {
-    uint64_t r = v[i].r;
+/* the outputs of the groups that start in [lo, hi) of the grouped order
+   (r ascending, then input index), written when write != 0 */
+static int64_t rotate_1q_range(const uint64_t* x, const cd* a, const uint64_t* r, const int64_t* idx,
+                               int64_t nnz, int64_t lo, int64_t hi, int qubit, const cd* U, uint64_t* x_out,
+                               cd* a_out, int write) {
+  const uint64_t m = 1ULL << qubit;
+  int64_t n = 0, i = lo;
+  while (i < hi) {
+    const uint64_t rr = r[i];
     int64_t j = i + 1;
-    while (j < nnz && v[j].r == r) ++j;
+    while (j < nnz && r[j] == rr) ++j;
     cd a0 = {0.0, 0.0}, a1 = {0.0, 0.0};
     for (int64_t t = i; t < j; ++t) {
-      int64_t oi = v[t].i;
+      const int64_t oi = idx[t];
       if (((x[oi] >> qubit) & 1ULL) == 0) a0 = a[oi]; else a1 = a[oi];
     }
     cd n0 = cd_add(cd_mul(U[0], a0), cd_mul(U[1], a1));
     cd n1 = cd_add(cd_mul(U[2], a0), cd_mul(U[3], a1));
-    if (hypot(n0.re, n0.im) > 1e-30) { x_out[n] = r; a_out[n] = n0; ++n; }
-    if (hypot(n1.re, n1.im) > 1e-30) { x_out[n] = r | m; a_out[n] = n1; ++n; }
+    if (hypot(n0.re, n0.im) > 1e-30) { if (write) { x_out[n] = rr; a_out[n] = n0; } ++n; }
+    if (hypot(n1.re, n1.im) > 1e-30) { if (write) { x_out[n] = rr | m; a_out[n] = n1; } ++n; }
     i = j;
   }
-  free(v);
+  return n;
+}
+int64_t orc_rotate_1q(const uint64_t* x, const cd* a, int64_t nnz, int qubit, const cd* U,
+                      uint64_t* x_out, cd* a_out) {
+  const uint64_t m = 1ULL << qubit;
+  uint64_t* r = (uint64_t*)malloc((size_t)(nnz > 0 ? nnz : 1) * sizeof(uint64_t));
+  int64_t* idx = (int64_t*)malloc((size_t)(nnz > 0 ? nnz : 1) * sizeof(int64_t));
+  const int T = par_threads_for(nnz);
+  int64_t* st = (int64_t*)calloc((size_t)T + 1, sizeof(int64_t));
+  int64_t* off = (int64_t*)calloc((size_t)T + 1, sizeof(int64_t));
+  if (!r || !idx || !st || !off) { free(r); free(idx); free(st); free(off); return -2; }
+#pragma omp parallel for num_threads(T) schedule(static)
+  for (int64_t i = 0; i < nnz; ++i) { r[i] = x[i] & ~m; idx[i] = i; }
+  /* group by x & ~m ascending; within a group, input order (a stable sort) */
+  if (par_radix_sort(r, idx, sizeof(int64_t), nnz)) { free(r); free(idx); free(st); free(off); return -2; }
+  /* ranges of whole groups: each range start moved forward to a group start */
+  for (int t = 0; t <= T; ++t) {
+    int64_t lo = par_lo(nnz, T, t);
+    while (lo > 0 && lo < nnz && r[lo] == r[lo - 1]) ++lo;
+    st[t] = lo;
+  }
+#pragma omp parallel num_threads(T)
+  {
+    const int t = par_tid();
+    off[t + 1] = rotate_1q_range(x, a, r, idx, nnz, st[t], st[t + 1], qubit, U, 0, 0, 0);
+  }
+  for (int t = 0; t < T; ++t) off[t + 1] += off[t];
+#pragma omp parallel num_threads(T)
+  {
+    const int t = par_tid();
+    rotate_1q_range(x, a, r, idx, nnz, st[t], st[t + 1], qubit, U, x_out + off[t], a_out + off[t], 1);
+  }
+  const int64_t n = off[T];
+  free(r); free(idx); free(st); free(off);
   return n;
 }
 
@@ -606,16 +847,8 @@ int64_t orc_rotate_2q(const uint64_t* x, const cd* a, int64_t nnz, int q1, int q
 /* ------------------------------------------------------------------ */
 /* reductions and fingerprints                                          */
 /* ------------------------------------------------------------------ */
-double orc_sum_p(const cd* a, int64_t n) {
-  i128 s = 0;
-  for (int64_t i = 0; i < n; ++i) s += fx_from(cd_p(a[i]));
-  return fx_to(s);
-}
-double orc_sum_p2(const cd* a, int64_t n) {
-  i128 s = 0;
-  for (int64_t i = 0; i < n; ++i) { double p = cd_p(a[i]); s += fx_from(p * p); }
-  return fx_to(s);
-}
+double orc_sum_p(const cd* a, int64_t n) { return fx_to(par_sum_p(a, n, 0)); }
+double orc_sum_p2(const cd* a, int64_t n) { return fx_to(par_sum_p(a, n, 1)); }
 /* exposes the accumulator for tests: exact sum of v[0..n) */
 double orc_exact_sum(const double* v, int64_t n) {
   i128 s = 0;

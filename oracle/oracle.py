@@ -45,10 +45,12 @@ C128 = np.complex128
 
 
 def build(force: bool = False) -> str:
-    """Compile bass_oracle.c into oracle/_build/liboracle.so (gcc, -O2, no FMA)."""
+    """Compile bass_oracle.c into oracle/_build/liboracle.so (gcc, -O2, no FMA,
+    OpenMP).  The heavy kernels run on ``set_threads(n)`` host threads (one by
+    default); their results do not depend on the thread count."""
     os.makedirs(os.path.dirname(_LIB_PATH), exist_ok=True)
     if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(_SRC):
-        cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+        cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
                "-o", _LIB_PATH, _SRC, "-lm"]
         subprocess.check_call(cmd)
     return _LIB_PATH
@@ -83,6 +85,8 @@ def lib():
             "orc_sum_p2": (D, [P, I64]),
             "orc_fingerprint": (None, [P, P, I64, D, P]),
             "orc_exact_sum": (D, [P, I64]),
+            "orc_threads": (I, []),
+            "orc_set_threads": (I, [I]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -90,6 +94,12 @@ def lib():
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def set_threads(n: int) -> int:
+    """Host threads for the oracle's kernels (n <= 0: every thread OpenMP
+    offers); returns the number in effect."""
+    return int(lib().orc_set_threads(int(n)))
 
 
 def _p(a: np.ndarray):
@@ -455,6 +465,52 @@ class OracleBASS:
             del self._kron_cache[key]
 
     # bass_simulator.py:730-827 (1-qubit passes)
+    def _descent_pass(self, st, qubits=None):
+        """One pass of the 1-qubit coordinate descent (bass_simulator.py:739-816):
+        the RDMs of the state, then a rotation step for every qubit in turn
+        (``qubits``: only those, for a bounded timing sample); returns whether
+        some rotation was kept."""
+        all_rho = rdm_all(st.x, st.alpha, self.N)
+        pr = self._pr(st)
+        improved = False
+        for j in (range(self.N) if qubits is None else qubits):
+            if self.use_fast_eigh:
+                _, V = eigh_2x2_py(all_rho[j])
+            else:
+                evals, V = np.linalg.eigh(all_rho[j])
+                V = V[:, np.argsort(-evals)]
+                if np.linalg.det(V).real < 0:
+                    V[:, 1] *= -1
+            if abs(V[0, 1]) + abs(V[1, 0]) < 1e-10:
+                continue
+            x_save, a_save, U_save = st.x, st.alpha, self.U[j].copy()
+            self.stats["rotations"] += 1
+            self.stats["amp_updates"] += st.nnz
+            st.x, st.alpha = rotate_1q(st.x, st.alpha, j, V.conj().T)
+            self._truncate_state(st)
+            frac = sum_p(st.alpha)
+            p2 = sum_p2(st.alpha)
+            self._renorm(st)
+            # PR of the renormalised candidate, from the exact sums of the
+            # unnormalised one: frac^2 / sum |a|^4 (the reference evaluates
+            # 1 / sum |a/sqrt(frac)|^4; the two differ by rounding only)
+            pr_new = (frac * frac) / p2 if (st.nnz > 0 and p2 > 0) else float("inf")
+            # the reference's rule is `pr_new >= pr`; a rotation must lower
+            # PR by more than pr_tie_tol (relative) to count (0 restores it)
+            if pr_new >= pr * (1.0 - self.pr_tie_tol):
+                st.x, st.alpha = x_save, a_save
+                self.U[j] = U_save
+            else:
+                self.U[j] = self.U[j] @ V
+                pr = pr_new
+                self._gamma_running *= np.sqrt(frac if frac > 1e-30 else 0)
+                self._invalidate_kron(j)
+                improved = True
+                self.stats["accepted"] += 1
+                if self.trace is not None:
+                    self.trace.accept(j)
+        return improved
+
     def _optimize_basis(self, st, gate_index=-1):
         if self._pr(st) < self.k / 4:
             return
@@ -462,46 +518,7 @@ class OracleBASS:
         if self.trace is not None:
             self.trace.opt(gate_index)
         for _pass in range(3):
-            all_rho = rdm_all(st.x, st.alpha, self.N)
-            pr = self._pr(st)
-            improved = False
-            for j in range(self.N):
-                if self.use_fast_eigh:
-                    _, V = eigh_2x2_py(all_rho[j])
-                else:
-                    evals, V = np.linalg.eigh(all_rho[j])
-                    V = V[:, np.argsort(-evals)]
-                    if np.linalg.det(V).real < 0:
-                        V[:, 1] *= -1
-                if abs(V[0, 1]) + abs(V[1, 0]) < 1e-10:
-                    continue
-                x_save, a_save, U_save = st.x, st.alpha, self.U[j].copy()
-                self.stats["rotations"] += 1
-                self.stats["amp_updates"] += st.nnz
-                st.x, st.alpha = rotate_1q(st.x, st.alpha, j, V.conj().T)
-                self._truncate_state(st)
-                frac = sum_p(st.alpha)
-                p2 = sum_p2(st.alpha)
-                self._renorm(st)
-                # PR of the renormalised candidate, from the exact sums of the
-                # unnormalised one: frac^2 / sum |a|^4 (the reference evaluates
-                # 1 / sum |a/sqrt(frac)|^4; the two differ by rounding only)
-                pr_new = (frac * frac) / p2 if (st.nnz > 0 and p2 > 0) else float("inf")
-                # the reference's rule is `pr_new >= pr`; a rotation must lower
-                # PR by more than pr_tie_tol (relative) to count (0 restores it)
-                if pr_new >= pr * (1.0 - self.pr_tie_tol):
-                    st.x, st.alpha = x_save, a_save
-                    self.U[j] = U_save
-                else:
-                    self.U[j] = self.U[j] @ V
-                    pr = pr_new
-                    self._gamma_running *= np.sqrt(frac if frac > 1e-30 else 0)
-                    self._invalidate_kron(j)
-                    improved = True
-                    self.stats["accepted"] += 1
-                    if self.trace is not None:
-                        self.trace.accept(j)
-            if not improved:
+            if not self._descent_pass(st):
                 break
         if self.use_2qubit_rotations and self.N >= 2:
             self._optimize_2q_pass(st, [(i, i + 1) for i in range(0, self.N - 1, 2)])

@@ -79,7 +79,7 @@ def test_batch_c64_matches_plain_c128(env):
     for (x, a, g, stats), st in zip(ref, got):
         assert st.alpha.dtype == np.complex64
         assert abs(np.vdot(st.alpha, st.alpha).real - 1.0) < 1e-6
-        if stats["accepted"]:
+        if stats["accepted"] or not all(np.array_equal(u, np.eye(2)) for u in st.U):
             # a basis rotation is kept when it lowers PR; float rounding moves
             # PR by ~1e-7 relative, so near-tie decisions can go the other way
             # and the two runs then follow different (equally valid)

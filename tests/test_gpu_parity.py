@@ -300,6 +300,8 @@ def test_bass_matches_oracle_exactly(B, orc, name):
     assert st.gamma == ost.gamma
     for j in range(int(z["N"])):
         assert np.array_equal(b.U[j], ob.U[j])
+    assert b.stats["amp_updates"] == ob.stats["amp_updates"]
+    assert b.stats["rotations"] == ob.stats["rotations"] and b.stats["accepted"] == ob.stats["accepted"]
 
 
 @pytest.mark.parametrize("name", BASS_CASES + LARGE_CASES)

@@ -55,5 +55,6 @@ def test_served_stream(env):
         assert alone.gamma == r.gamma
         b = BASS(n, k)
         plain = b.simulate(circ)
-        if not b.stats["accepted"]:   # without basis rotations the runs are comparable entry by entry
+        # without basis rotations (on either side) the runs are comparable entry by entry
+        if not b.stats["accepted"] and all(np.array_equal(u, np.eye(2)) for u in alone.U):
             assert _fid(plain.x, plain.alpha, r.x, r.alpha) >= 1 - 1e-6
