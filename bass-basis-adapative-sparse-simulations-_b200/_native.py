@@ -231,8 +231,14 @@ class Engine:
               "bass_ctrl_init")
 
     def read_ctrl(self):
-        """Synchronising read of the control block (numpy record)."""
-        return np.frombuffer(self.ctrl.cpu().numpy().tobytes(), dtype=CTRL_DTYPE)[0]
+        """Synchronising read of the control block (numpy record), through a
+        pinned host buffer."""
+        torch = self.torch
+        if getattr(self, "_ctrl_host", None) is None:
+            self._ctrl_host = torch.empty(self.ctrl.numel(), dtype=torch.uint8, pin_memory=True)
+        self._ctrl_host.copy_(self.ctrl, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return np.frombuffer(self._ctrl_host.numpy().tobytes(), dtype=CTRL_DTYPE)[0]
 
     def ctrl_field(self, name, np_dtype):
         off = CTRL_DTYPE.fields[name][1]
@@ -240,11 +246,18 @@ class Engine:
         return self.ctrl[off:off + size]
 
     def set_ctrl(self, name, value):
-        """Asynchronous write of one scalar control field."""
+        """Asynchronous write of one scalar control field: a fill of the field
+        on the stream (no host synchronisation)."""
+        torch = self.torch
         dt = CTRL_DTYPE.fields[name][0]
-        b = np.array([value], dtype=dt).view(np.uint8)
         off = CTRL_DTYPE.fields[name][1]
-        self.ctrl[off:off + len(b)].copy_(self.torch.from_numpy(b.copy()), non_blocking=False)
+        view = {np.dtype("<f8"): torch.float64, np.dtype("<i8"): torch.int64, np.dtype("<u8"): torch.int64,
+                np.dtype("<i4"): torch.int32, np.dtype("<u4"): torch.int32}.get(np.dtype(dt))
+        if view is None:
+            raise TypeError(f"control field {name} is not a scalar")
+        if np.dtype(dt).kind == "u":   # same bits through the signed view
+            value = int(np.array([value], dtype=dt).view(np.dtype(dt).str.replace("u", "i"))[0])
+        self.ctrl[off:off + np.dtype(dt).itemsize].view(view).fill_(value)
 
     def check_errors(self):
         """Synchronising read of the control block; raises on a device error."""

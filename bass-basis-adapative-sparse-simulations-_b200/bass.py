@@ -87,9 +87,10 @@ class BASS:
         return state._pr() > self._pr_at_last_opt / self.pr_opt_threshold
 
     # bass_simulator.py:730-827 (1-qubit coordinate descent)
-    def _optimize_basis(self, state, gate_index=-1):
+    def _optimize_basis(self, state, gate_index=-1, pr=None):
+        """pr: the state's PR when the caller has just computed it."""
         eng = state._eng
-        if state._pr() < self.k / 4:
+        if (state._pr() if pr is None else pr) < self.k / 4:
             return
         self.stats["opt_calls"] += 1
         if self.trace:
@@ -241,11 +242,20 @@ class BASS:
         return n
 
     def _maybe_optimize(self, state, i, M):
+        """bass_simulator.py:917-925: every optimize_every gates, if a
+        truncation happened since the last check and PR has grown past the
+        trigger (optimize_trigger), optimise the basis.  The PR reduction is
+        launched before the one synchronising read of the control block, so
+        the flag and the PR arrive together."""
         if self.optimize_every > 0 and (i + 1) % self.optimize_every == 0 and i + 1 < M:
             eng = state._eng
-            if int(eng.read_ctrl()["truncation_active"]) and self.optimize_trigger(state):
-                self._optimize_basis(state, i)
-                self._pr_at_last_opt = state._pr()
+            nat.check(eng.L.bass_pr(state._cur.ptr, eng.ctrl_ptr, eng.ws_ptr, eng.ws_bytes, eng.stream), "bass_pr")
+            c = eng.read_ctrl()
+            if int(c["truncation_active"]):
+                pr = float(c["pr_last"])
+                if self.pr_opt_threshold >= 1.0 or pr > self._pr_at_last_opt / self.pr_opt_threshold:
+                    self._optimize_basis(state, i, pr=pr)
+                    self._pr_at_last_opt = state._pr()
             eng.set_ctrl("truncation_active", 0)
 
     # bass_simulator.py:608-621

@@ -707,12 +707,35 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
       uint16_t rp[kPerThread];
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) rp[k] = (d + k < E) ? sIdx[rs[k]] : 0;
+      // Each thread writes its kPerThread consecutive positions in a skewed
+      // order, starting at element sk = (lane / 2) mod 8: the 16 lanes of a
+      // half-warp then hit 16 different bank pairs with their 8-byte stores
+      // (in plain order they hit two).  The registers are rotated by sk
+      // first (a fixed network of selects, no dynamic register indexing).
+      static_assert(kPerThread == 8, "skewed write-back of eight positions");
+      const int sk = (lane >> 1) & 7;
+#pragma unroll
+      for (int b = 1; b < kPerThread; b <<= 1) {
+        uint64_t tz[kPerThread];
+        uint16_t tp[kPerThread];
+#pragma unroll
+        for (int k = 0; k < kPerThread; ++k) {
+          tz[k] = (sk & b) ? rz[(k + b) & 7] : rz[k];
+          tp[k] = (sk & b) ? rp[(k + b) & 7] : rp[k];
+        }
+#pragma unroll
+        for (int k = 0; k < kPerThread; ++k) {
+          rz[k] = tz[k];
+          rp[k] = tp[k];
+        }
+      }
       __syncthreads();
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
-        if (d + k < E) {
-          sZ[d + k] = rz[k];
-          sPerm[d + k] = rp[k];  // the amplitudes stay where they were loaded (sIdx was read above)
+        const int pos = d + ((k + sk) & 7);   // rz[k] now holds position d + (k + sk) mod 8
+        if (pos < E) {
+          sZ[pos] = rz[k];
+          sPerm[pos] = rp[k];  // the amplitudes stay where they were loaded (sIdx was read above)
         }
       }
       __syncthreads();

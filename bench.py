@@ -456,6 +456,19 @@ def overlap_fidelity(x1, a1, x2, a2):
     return float(abs(ov) ** 2 / (n1 * n2)) if n1 > 0 and n2 > 0 else 0.0
 
 
+def perturbed_fidelity(pkg, spec, circ, ref_state, eps):
+    """Fidelity between ref_state (BASS complex128 on circ) and BASS complex128
+    on circ with its first 1-qubit gate preceded by an X rotation of eps rad."""
+    import numpy as np
+    from bass_b200.bass import BASS
+    c2 = list(circ)
+    j = next(t for t, g in enumerate(c2) if g.n_qubits == 1)
+    R = np.array([[np.cos(eps), -1j * np.sin(eps)], [-1j * np.sin(eps), np.cos(eps)]])
+    c2[j] = pkg.gates.QuantumGate(c2[j].qubits, R @ c2[j].matrix)
+    st = BASS(*spec).simulate(c2)
+    return overlap_fidelity(ref_state.x, ref_state.alpha, st.x, st.alpha)
+
+
 def identity_frames(U):
     """Every frame of a finished batched / served state is the identity."""
     import numpy as np
@@ -553,7 +566,7 @@ def form_batched(a, pkg):
     nd = min(64, len(specs))
     specs_d, circs_d = pkg.circuits.config4_batch(seed=a.seed + 1, count=nd, disorder_h=0.25)
     got_d = BatchedBASS(specs_d, dtype=np.complex64).simulate(circs_d)
-    fd, split = [], 0
+    fd, split, low = [], 0, []
     for i in range(nd):
         b = BASS(*specs_d[i])
         st = b.simulate(circs_d[i])
@@ -561,6 +574,15 @@ def form_batched(a, pkg):
         split += (not b.stats["accepted"]) != identity_frames(got_d[i].U)
         if same:
             fd.append(overlap_fidelity(st.x, st.alpha, got_d[i].x, got_d[i].alpha))
+            if fd[-1] < 1 - 1e-6:
+                rec = {"n": specs_d[i][0], "K": specs_d[i][1], "gates": len(circs_d[i]),
+                       "truncations": int(b.stats["truncations"]), "fidelity": fd[-1]}
+                if len(low) < 4:
+                    # the same complex128 run with the first 1-qubit gate turned by a further
+                    # 1e-7 rad about X: how far the truncated evolution carries a perturbation
+                    # of the size of complex64 rounding
+                    rec["complex128_perturbed_1e-7"] = perturbed_fidelity(pkg, specs_d[i], circs_d[i], st, 1e-7)
+                low.append(rec)
     return {"form": "batched", "workload": f"{len(specs)} TFIM circuits, n~U[16,48], layers~U[10,60], "
                                            "h~U[0.3,2], dt=0.05, K=2^U[10,20] (config 4)",
             "batched_complex64": {"circuits_per_s": batch_cps, "seconds": t_batch,
@@ -572,7 +594,7 @@ def form_batched(a, pkg):
             "fidelity_below_1e-6": sum(1 for f in comparable if f < 1 - 1e-6),
             "tie_free": {"circuits": nd, "compared": len(fd), "fidelity_min": min(fd) if fd else None,
                          "fidelity_below_1e-6": sum(1 for f in fd if f < 1 - 1e-6),
-                         "rotation_decisions_differ": split,
+                         "rotation_decisions_differ": split, "below": low[:12],
                          "note": "config-4 distribution with site fields h_i ~ U[h - 0.25, h + 0.25]"},
             "fidelity_note": "compared entry by entry where neither run kept a basis rotation (both in the "
                              "computational basis); a run that kept one holds its state in another frame, and "
