@@ -908,7 +908,7 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
       uint64_t kb;
       double2 ca[NS];
       unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.ws.tmp_keys) + NS * sZstart;
-      uint64_t* skeys = a.ws.stage_keys + NS * sZstart;
+      uint64_t* skeys = a.ws.stage_keys + sZstart;  // one base key per Z position (staged_key)
       double2* samps = a.ws.tmp_amps + NS * sZstart;
       float2* sampf = reinterpret_cast<float2*>(a.ws.tmp_amps) + NS * sZstart;
       for (int p = tid; p < E; p += kThreads) {
@@ -924,15 +924,11 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
           }
         }
         if (cm) {  // every slot of the group is written (a missing child's slot holds ~0 bits)
+          skeys[p] = kb;
           if (NS == 1) {
-            skeys[p] = kb;
             if (c64) sampf[p] = d2f(ca[0]);
             else samps[p] = ca[0];
           } else {
-#pragma unroll
-            for (int c = 0; c < NS; c += 2)
-              *reinterpret_cast<ulonglong2*>(skeys + (long long)NS * p + c) =
-                  make_ulonglong2(kb | (uint64_t)c, kb | (uint64_t)(c + 1));
             if (c64) {
 #pragma unroll
               for (int c = 0; c < NS; c += 2) {
@@ -1206,10 +1202,20 @@ __device__ void sort_pairs(unsigned long long* sb, unsigned long long* sk, unsig
   }
 }
 
-// The true key of the child staged at slot i (qat: the op's output order).
-__device__ __forceinline__ unsigned long long cand_true_key(const OpArgs& a, unsigned long long i,
+// The physical key of the child staged at slot i: the evaluation pass stages
+// one key per Z position, its group's base key (low lns bits clear), and
+// child c of the group sits at slot (position << lns) | c.
+__device__ __forceinline__ uint64_t staged_key(const uint64_t* sk, unsigned long long i, int lns, bool streaming) {
+  const unsigned long long p = i >> lns;
+  const uint64_t base = streaming ? __ldcs(sk + p) : __ldcg(sk + p);
+  return base | (uint64_t)(i & ((1ULL << lns) - 1));
+}
+
+// The true key of the child staged at slot i (qat: the op's output order,
+// lns: log2 of the slots per entry).
+__device__ __forceinline__ unsigned long long cand_true_key(const OpArgs& a, unsigned long long i, int lns,
                                                             const int8_t* qat) {
-  return true_key(__ldcg(a.ws.stage_keys + i), qat, 64);
+  return true_key(staged_key(a.ws.stage_keys, i, lns, false), qat, 64);
 }
 
 // The threshold of the level-2 boundary bin's m candidates (slot indices in
@@ -1217,8 +1223,8 @@ __device__ __forceinline__ unsigned long long cand_true_key(const OpArgs& a, uns
 // desc, true key asc) gives (t_bits, t_key); t_key is ~0 when every candidate
 // at t_bits is kept.  The candidates stay in shared memory (bits, true key,
 // slot index: three arrays of kCandSmem words, in some order) for the caller.
-__device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, long long need, const int8_t* qat,
-                             unsigned long long* tb_out, unsigned long long* tk_out) {
+__device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, long long need, int lns,
+                             const int8_t* qat, unsigned long long* tb_out, unsigned long long* tk_out) {
   unsigned long long* sb = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* sk = sb + kCandSmem;
   unsigned long long* ssi = sk + kCandSmem;
@@ -1228,7 +1234,7 @@ __device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, 
     const unsigned long long si = __ldcg(a.ws.cand_bits + i);
     ssi[i] = si;
     sb[i] = __ldcg(slots + si);
-    sk[i] = cand_true_key(a, si, qat);
+    sk[i] = cand_true_key(a, si, lns, qat);
   }
   __syncthreads();
   const long long r = need < 1 ? 0 : (need > m ? m - 1 : need - 1);
@@ -1260,7 +1266,7 @@ __device__ void settle_small(const OpArgs& a, unsigned char* smem, long long m, 
 // low 37 bits of the bit pattern (the 26-bit prefix pre is shared), then, if
 // the cut falls inside a run of equal patterns, on the true keys of that run.
 __device__ void settle_radix(const OpArgs& a, unsigned char* smem, long long m, long long need,
-                             unsigned long long pre, const int8_t* qat, unsigned long long* tb_out,
+                             unsigned long long pre, int lns, const int8_t* qat, unsigned long long* tb_out,
                              unsigned long long* tk_out) {
   unsigned int* h = reinterpret_cast<unsigned int*>(smem);
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
@@ -1309,7 +1315,7 @@ __device__ void settle_radix(const OpArgs& a, unsigned char* smem, long long m, 
     for (long long i = tid; i < m; i += blockDim.x) {
       const unsigned long long si = __ldcg(a.ws.cand_bits + i);
       if (__ldcg(slots + si) != tb) continue;
-      const unsigned long long k = cand_true_key(a, si, qat);
+      const unsigned long long k = cand_true_key(a, si, lns, qat);
       if (shift == 56 || (k >> (shift + 8)) == p) atomicAdd(&h[(unsigned)(k >> shift) & 255u], 1u);
     }
     __syncthreads();
@@ -1501,21 +1507,21 @@ __device__ void settle_boundary(const OpArgs& a, int ns, int kind, unsigned long
     if (tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
     m = a.ws.max_n;
   }
+  const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;
   unsigned long long tb, tk;
-  if (m <= kCandSmem) settle_small(a, smem, m, lneed, qat, &tb, &tk);
-  else settle_radix(a, smem, m, lneed, lpre, qat, &tb, &tk);
+  if (m <= kCandSmem) settle_small(a, smem, m, lneed, lns, qat, &tb, &tk);
+  else settle_radix(a, smem, m, lneed, lpre, lns, qat, &tb, &tk);
   if (tid == 0) {
     sel->t_bits = tb;
     sel->t_key = tk;
   }
   const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
-  const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;
   const bool in_smem = m <= kCandSmem;  // settle_small left (bits, key, slot) there
   const unsigned long long* sb = reinterpret_cast<const unsigned long long*>(smem);
   for (long long k = tid; k < m; k += blockDim.x) {
     const unsigned long long i = in_smem ? sb[2 * kCandSmem + k] : __ldcg(a.ws.cand_bits + k);
     const unsigned long long bits = in_smem ? sb[k] : __ldcg(slots + i);
-    if (bits > tb || (bits == tb && (in_smem ? sb[kCandSmem + k] : cand_true_key(a, i, qat)) <= tk)) {
+    if (bits > tb || (bits == tb && (in_smem ? sb[kCandSmem + k] : cand_true_key(a, i, lns, qat)) <= tk)) {
       atomicAdd(reinterpret_cast<unsigned long long*>(a.ws.status + tile_of((long long)(i >> lns), kind, a.ws.part)),
                 1ULL);
       vk[0] += fx_from_pbits(bits);
@@ -1807,6 +1813,7 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
   const float2* stf = reinterpret_cast<const float2*>(a.ws.tmp_amps);
   constexpr bool c64 = C64;
   const long long cap = a.out->cap;
+  const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;
   const unsigned lt = (1u << lane) - 1;
   long long written = 0;
   for (long long b = g.bid; ok && !S.skip_write && b < ntiles; b += g.nblk) {
@@ -1842,7 +1849,8 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
       // children tied at the threshold pattern: kept up to the true key t_key
       for (unsigned r = tm; r; r &= r - 1) {
         const int u = __ffs(r) - 1;
-        if (true_key(__ldcs(a.ws.stage_keys + i0 + u * kThreads + tid), S.qat, 64) <= S.t_key) km |= 1u << u;
+        if (true_key(staged_key(a.ws.stage_keys, i0 + u * kThreads + tid, lns, true), S.qat, 64) <= S.t_key)
+          km |= 1u << u;
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
@@ -1850,7 +1858,7 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
         const bool kept = (km >> u) & 1u;
         bal[u] = __ballot_sync(0xffffffffu, kept);
         if (kept) {
-          kk[u] = __ldcs(a.ws.stage_keys + i);
+          kk[u] = staged_key(a.ws.stage_keys, i, lns, true);
           if (c64) {
             const float2 f = __ldcs(stf + i);
             aa[u] = make_double2(f.x, f.y);
