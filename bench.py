@@ -193,7 +193,7 @@ def run_reference(a, rank, world):
 
 
 def workload_config(a):
-    return {"workload": f"BASS brickwork n={a.n} depth={a.depth} K=2^{a.k.bit_length() - 1} complex128",
+    return {"workload": f"BASS brickwork n={a.n} depth={a.depth} K=2^{a.k.bit_length() - 1} {a.dtype}",
             "n_qubits": a.n, "depth": a.depth, "K": a.k, "optimize_every": 5, "buffer_factor": 2,
             "parallelism": f"replicas x{a.gpus}", "l2": "flushed between steps (512 MB write)"}
 
@@ -218,8 +218,10 @@ def run_ours(a, rank, world, dist):
         if dist is not None:
             dist.barrier()
 
+    dt = np.dtype(a.dtype)
+
     def step():
-        b = BASS(a.n, a.k)
+        b = BASS(a.n, a.k, dtype=dt)
         st = b.simulate(circ)
         return b, st
 
@@ -255,7 +257,7 @@ def run_ours(a, rank, world, dist):
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
-        b = BASS(a.n, a.k)
+        b = BASS(a.n, a.k, dtype=dt)
         st = b.simulate(circ)
         x, al = st.x, st.alpha
         t1 = time.perf_counter()
@@ -281,7 +283,7 @@ def run_ours(a, rank, world, dist):
         line = {
             "metric": "amp_updates_per_s", "value": value, "unit": "amp-updates/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t_total / a.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": a.dtype,
             "data": "synthetic (seeded brickwork circuit)", "config": workload_config(a),
             "e2e": {"value": e2e_value, "unit": "amp-updates/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
@@ -299,8 +301,9 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
     ms = np.zeros(nat.PROF_SLOTS)
     cnt = np.zeros(nat.PROF_SLOTS, dtype=np.int64)
     L.bass_profile_collect(nat._host(ms), nat._host(cnt), nat.PROF_SLOTS)
-    b = BASS(a.n, a.k)
+    b = BASS(a.n, a.k, dtype=np.dtype(a.dtype))
     st = b.simulate(circ)
+    be = 24 if np.dtype(a.dtype) == np.complex128 else 16   # bytes per entry
     torch.cuda.synchronize()
     c = st._eng.read_ctrl()
     L.bass_profile_collect(nat._host(ms), nat._host(cnt), nat.PROF_SLOTS)
@@ -313,14 +316,14 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
     for s in np.argsort(-ms):
         if ms[s] <= 0:
             break
-        nbytes = 24 * (int(c["prof_in"][s]) + int(c["prof_out"][s]))
+        nbytes = be * (int(c["prof_in"][s]) + int(c["prof_out"][s]))
         kernels.append({"kernel": nat.SLOT_NAMES[s], "ms": round(float(ms[s]), 3), "launches": int(cnt[s]),
                         "share": round(float(ms[s] / ms.sum()), 4),
                         "gbs": round(nbytes / (ms[s] * 1e-3) / 1e9, 1) if nbytes else None})
     phases = select_phases(c, nat)
     tile_slots = [s for s in range(30) if ms[s] > 0]
     dom = max(tile_slots, key=lambda s: ms[s])
-    per_launch_bytes = 24 * (int(c["prof_in"][dom]) + int(c["prof_out"][dom])) / cnt[dom]
+    per_launch_bytes = be * (int(c["prof_in"][dom]) + int(c["prof_out"][dom])) / cnt[dom]
     avg_s = ms[dom] * 1e-3 / cnt[dom]
     achieved = per_launch_bytes / avg_s / 1e9
     traffic = None
@@ -328,12 +331,12 @@ def profile_step(a, circ, L, nat, BASS, torch, step_ms):
     if os.path.exists(tfile):
         tj = json.load(open(tfile))
         if nat.SLOT_NAMES[dom] in tj:
-            traffic = tj[nat.SLOT_NAMES[dom]] * per_launch_bytes / 24
+            traffic = tj[nat.SLOT_NAMES[dom]] * per_launch_bytes / be if be == 24 else None
     # the whole simulate call: every gate / rotation / truncation reads its
     # input once and writes its output once (24 B per entry each way), over
     # the timed step's duration (RDMs, selection, partitions all included)
     kinds = (0, 1, 2, 4)  # gate1, rot1, gate2, plain; the 2-qubit gate's first pass is overhead
-    step_bytes = 24 * (sum(int(c["prof_in"][k * 5 + 0]) for k in kinds) +
+    step_bytes = be * (sum(int(c["prof_in"][k * 5 + 0]) for k in kinds) +
                        sum(int(c["prof_out"][k * 5 + 3]) for k in kinds))
     step_gbs = step_bytes / (step_ms * 1e-3) / 1e9
     top = int(np.argmax(ms))  # the longest kernel overall (the selection has no algorithmic bytes of its own)
@@ -577,7 +580,7 @@ def form_batched(a, pkg):
             if fd[-1] < 1 - 1e-6:
                 rec = {"n": specs_d[i][0], "K": specs_d[i][1], "gates": len(circs_d[i]),
                        "truncations": int(b.stats["truncations"]), "fidelity": fd[-1]}
-                if len(low) < 4:
+                if len(low) < 8:
                     # the same complex128 run with the first 1-qubit gate turned by a further
                     # 1e-7 rad about X: how far the truncated evolution carries a perturbation
                     # of the size of complex64 rounding

@@ -91,6 +91,20 @@ def test_batch_c64_matches_plain_c128(env):
     assert checked >= len(specs) // 2
 
 
+def test_batch_c64_equals_plain_c64(env):
+    # the segmented launches compute what the single-state launches compute,
+    # in complex64 as in complex128: bit for bit
+    from bass_b200.bass import BASS
+    from bass_b200.batch import BatchedBASS
+    specs, circs = _mix(env, disorder_h=0.25)
+    got = BatchedBASS(specs, dtype=np.complex64).simulate(circs)
+    for (n, k), c, st in zip(specs, circs, got):
+        b = BASS(n, k, dtype=np.complex64)
+        p = b.simulate(c)
+        assert np.array_equal(p.x, st.x) and np.array_equal(p.alpha, st.alpha)
+        assert p.gamma == st.gamma
+
+
 def test_batch_result_same_alone_and_in_mix(env):
     from bass_b200.batch import BatchedBASS
     specs, circs = _mix(env)
