@@ -1004,7 +1004,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(const __grid_constant__ Op
 // kept true key t_key; the write step applies the same rule.  The grid
 // barrier is a counter and a generation word in the
 // workspace with a bounded spin (BASS_ERR_WAIT, then every block returns).
-constexpr int kSelThreads = 512;
+constexpr int kSelThreads = 1024;
 // dynamic shared memory of the selection: the histograms (kHistBins words),
 // later the boundary candidates (bits, true key, slot index)
 constexpr size_t kSelSmem = (size_t)kCandSmem * 24;
