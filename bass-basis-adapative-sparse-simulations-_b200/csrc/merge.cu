@@ -1010,36 +1010,34 @@ constexpr int kSelThreads = 1024;
 constexpr size_t kSelSmem = (size_t)kCandSmem * 24;
 
 // Grid-wide barrier of the selection's grid (every block resident, see
-// launch_select_t).  Returns false (error recorded) if the wait gave up.
-__device__ bool grid_sync(const OpArgs& a, Grp gr) {
+// launch_select_t).  An arrival counter that only grows within the kernel
+// (the op's workspace clear zeroes it): the b-th barrier of a block adds one
+// (release) and waits until the counter reaches b x blocks (acquire), so no
+// arrival waits for an atomic's result and no last block has to publish a
+// release.  Every block passes the same barriers in the same order; gen is
+// the block's count of barriers passed (shared memory, zero at the start of
+// the kernel).  Returns false (error recorded) if the wait gave up.
+__device__ bool grid_sync(const OpArgs& a, Grp gr, unsigned long long& gen) {
   __shared__ int sOk;
   __syncthreads();
   if (threadIdx.x == 0) {
-    // arrival counter and generation word on separate cache lines, so that
-    // the waiting blocks' polling does not slow down the arrivals
     unsigned long long* cnt = reinterpret_cast<unsigned long long*>(a.ws.counters) + 60;
-    unsigned long long* gen = reinterpret_cast<unsigned long long*>(a.ws.counters) + 32;
-    const unsigned long long g = ld_acquire(gen);
+    const unsigned long long target = (gen + 1) * (unsigned long long)gr.nblk;
     __threadfence();
-    const unsigned long long arrived = atomicAdd(cnt, 1ULL);
+    red_release_add(cnt, 1ULL);
     int ok = 1;
-    if (arrived == (unsigned long long)gr.nblk - 1) {
-      atomicExch(cnt, 0ULL);
-      __threadfence();
-      st_release(gen, g + 1);
-    } else {
-      long long spins = 0;
-      const long long lim = wait_limit(a.ctrl);
-      while (ld_acquire(gen) == g) {
-        if (++spins > lim) {
-          set_error(a.ctrl, BASS_ERR_WAIT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(32);
+    long long spins = 0;
+    const long long lim = wait_limit(a.ctrl);
+    while (ld_acquire(cnt) < target) {
+      if (++spins > lim) {
+        set_error(a.ctrl, BASS_ERR_WAIT);
+        ok = 0;
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
+    gen += 1;
     sOk = ok;
   }
   __syncthreads();
@@ -1671,6 +1669,7 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
   __shared__ long long sS[kSelThreads / 32];
   __shared__ i128 sRed[3 * (kSelThreads / 32)];
   __shared__ long long sNout;
+  __shared__ unsigned long long sBarGen;  // grid barriers passed by this block
   __shared__ int8_t sQat[64];
   SelState* sel = a.ws.sel;
   const int tid = threadIdx.x;
@@ -1699,6 +1698,7 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
     long long s = 0;
     for (int w = 0; w < kSelThreads / 32; ++w) s += sS[w];
     sNout = s;
+    sBarGen = 0ULL;
   }
   __syncthreads();
   const long long n_out = sNout;
@@ -1716,7 +1716,7 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
   } else if (trunc) {
     // 2. radix select on the bit patterns
     slot_hist_phase<1>(slots, nslots, 0, h, a.ws.hist1, g);
-    if (!grid_sync(a, g)) return;
+    if (!grid_sync(a, g, sBarGen)) return;
     long long c_gt, c_b1;
     const int b1 = find_bin(a.ws.hist1, a.k_keep, &c_gt, &c_b1);
     const long long need = a.k_keep - c_gt;
@@ -1726,7 +1726,7 @@ __device__ __forceinline__ void select_body(const OpArgs& a, Grp g, int ns, int 
     } else {
       two = 1;
       slot_hist_phase<2>(slots, nslots, (unsigned long long)b1, h, a.ws.hist2, g);
-      if (!grid_sync(a, g)) return;
+      if (!grid_sync(a, g, sBarGen)) return;
       long long c_gt2, c_b2;
       const int b2 = find_bin(a.ws.hist2, need, &c_gt2, &c_b2);
       const long long need2 = need - c_gt2;
