@@ -31,7 +31,7 @@ constexpr int kHistBins = 8192;      // 13-bit radix-select digits
 constexpr int kGroupBins = 128;      // bins per coarse group of a selection histogram
 constexpr int kHistGroups = kHistBins / kGroupBins;  // coarse counts stored after the bins
 constexpr int kCandSmem = 4096;      // candidates sorted in shared memory
-constexpr int kRankMax = 256;        // candidates ranked by direct counting
+constexpr int kRankMax = 1024;       // candidates ranked by direct counting (one per thread of a selection block)
 constexpr int kMaxSets = 64;         // partition sets (one per qubit for RDMs)
 constexpr int kFxFrac = 96;
 constexpr long long kSpinLimit = 1LL << 22;  // a few seconds at most
