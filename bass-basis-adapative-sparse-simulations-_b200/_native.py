@@ -109,6 +109,7 @@ def load_library():
     sig = {
         "bass_version": (ctypes.c_char_p, []),
         "bass_state_bytes": (SZ, []),
+        "bass_batch_max_segments": (I32, []),
         "bass_ctrl_bytes": (SZ, []),
         "bass_workspace_bytes": (SZ, [I64, I64, I32]),
         "bass_state_init": (I32, [P, P, P, I64, I32, ctypes.c_uint64, P]),

@@ -32,7 +32,7 @@ from . import _native as nat
 from .linalg import eigh_2x2_many, kron_2x2
 from .state import SparseState
 
-MAX_SEG = 256   # ops that truncate or rotate keep every selection block resident
+MAX_SEG = 256   # resident circuits of a pool (a launch takes bass_batch_max_segments() of them)
 
 
 def gate_arrays(circuit):
@@ -87,7 +87,10 @@ class StatePool:
         # every slot's control block and RDM moments are contiguous: one read covers them all
         self.ctrl_all = torch.zeros((S, cb), dtype=torch.uint8, device=self.device)
         self.rho_all = torch.zeros((S, 4 * 64), dtype=torch.float64, device=self.device)
-        self.bws_bytes = int(self.L.bass_batch_ws_bytes(MAX_SEG))
+        # a segmented selection keeps one block group per state resident: a
+        # launch takes at most this many states (one selection block per SM)
+        self.seg_chunk = max(1, min(MAX_SEG, int(self.L.bass_batch_max_segments())))
+        self.bws_bytes = int(self.L.bass_batch_ws_bytes(self.seg_chunk))
         self.bws = torch.empty(self.bws_bytes, dtype=torch.uint8, device=self.device)
         self.stream = nat.ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
         self.states = [None] * S
@@ -192,8 +195,8 @@ class StatePool:
 
     def _call(self, name, o, *extra):
         f = getattr(self.L, name)
-        for part in range(0, len(o), MAX_SEG):
-            chunk = np.ascontiguousarray(o[part:part + MAX_SEG])
+        for part in range(0, len(o), self.seg_chunk):
+            chunk = np.ascontiguousarray(o[part:part + self.seg_chunk])
             nat.check(f(nat.ctypes.c_void_p(chunk.ctypes.data), len(chunk), *extra,
                         nat.ctypes.c_void_p(nat._ptr(self.bws)), self.bws_bytes, self.stream), name)
         self.stats["launch_calls"] += 1

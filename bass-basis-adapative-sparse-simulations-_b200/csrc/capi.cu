@@ -56,19 +56,21 @@ ProfScope::~ProfScope() {
 }
 
 const Device& device() {
-  static Device d = [] {
+  static Device d[kMaxDevices + 1];
+  static std::once_flag once[kMaxDevices + 1];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = kMaxDevices;
+  std::call_once(once[dev], [dev] {
     Device x{};
-    int dev = 0;
-    cudaGetDevice(&dev);
     int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (dev < kMaxDevices) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     x.sms = sms > 0 ? sms : 1;
     x.grid_small = x.sms * 8;
     x.grid_tile = x.sms * 2;
     x.grid_tile_h = x.sms;
-    return x;
-  }();
-  return d;
+    d[dev] = x;
+  });
+  return d[dev];
 }
 
 // ---------------------------------------------------------------------------
@@ -567,6 +569,12 @@ static int same_type(const std::vector<OpArgs>& v) {
 }  // namespace bass
 
 extern "C" {
+
+int bass_batch_max_segments(void) {
+  int n = 0;
+  if (seg_max_segments(&n) != cudaSuccess) return 0;
+  return n < kMaxSeg ? n : kMaxSeg;
+}
 
 size_t bass_batch_ws_bytes(int max_ops) {
   if (max_ops < 1) max_ops = 1;

@@ -1,6 +1,8 @@
 // internal.h -- host-side launchers shared by the .cu files of libbass_b200.
 #pragma once
 
+#include <atomic>
+#include <mutex>
 #include <utility>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -97,7 +99,30 @@ struct Device {
   int grid_tile_h;  // ... of the histogram passes (more shared memory)
   int grid_small;
 };
+// The current device's properties (looked up once per device).
 const Device& device();
+
+// A launch-configuration value (a kernel's resident grid) worked out once per
+// device: it depends only on the device, so racing first computations store
+// the same value.
+constexpr int kMaxDevices = 64;
+struct PerDevice {
+  std::atomic<int> v[kMaxDevices];
+};
+template <typename F>
+inline cudaError_t per_device(PerDevice& c, int* out, F compute) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return compute(out);
+  int x = c.v[dev].load(std::memory_order_acquire);
+  if (x == 0) {
+    if ((e = compute(&x)) != cudaSuccess) return e;
+    c.v[dev].store(x, std::memory_order_release);
+  }
+  *out = x;
+  return cudaSuccess;
+}
 
 bool carve(void* ws, size_t ws_bytes, WsView* v);
 // 1 if the state was set up (bass_state_init_typed / import / copy_desc) with
@@ -130,6 +155,8 @@ cudaError_t run_commit(bass_state* cur, bass_state* tmp, bass_ctrl* ctrl, const 
 cudaError_t run_merge_op_seg(int kind, const OpArgs* ops_dev, int nseg, int c64, int fin_mode, int trace,
                              SegPlan* plan_dev, cudaStream_t s);
 cudaError_t run_rdm_seg(const OpArgs* ops_dev, int nseg, int max_nq, int c64, SegPlan* plan_dev, cudaStream_t s);
+// the most segments one segmented launch takes on the current device
+cudaError_t seg_max_segments(int* out);
 // misc.cu, segmented: diagonal 2-qubit phases; PR (mode 1) or renormalisation (mode 0)
 cudaError_t run_phase2q_seg(const OpArgs* ops_dev, int nseg, int c64, cudaStream_t s);
 cudaError_t run_reduce_seg(const OpArgs* ops_dev, int nseg, int mode, int c64, cudaStream_t s);

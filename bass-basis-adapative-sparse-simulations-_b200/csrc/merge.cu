@@ -1967,19 +1967,18 @@ __global__ void k_rdm_final(const bass_state* st, double* rho, WsView ws, int fi
 template <int KIND, int PASS, bool C64>
 static cudaError_t tile_grid(size_t* smem_out, int* grid_out) {
   const size_t smem = (size_t)kTilePad * (16 + 8 + 2 + (PASS == P_WRITE ? 3 : 0));
-  static int grid = 0;
-  if (grid == 0) {
+  static PerDevice cache;
+  *smem_out = smem;
+  return per_device(cache, grid_out, [smem](int* grid) {
     cudaError_t e = cudaFuncSetAttribute(k_tile<KIND, PASS, C64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int occ = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<KIND, PASS, C64>, kThreads, smem);
     if (e != cudaSuccess) return e;
-    grid = device().sms * (occ > 0 ? occ : 1);
-    if (grid > 1024) grid = 1024;
-  }
-  *smem_out = smem;
-  *grid_out = grid;
-  return cudaSuccess;
+    *grid = device().sms * (occ > 0 ? occ : 1);
+    if (*grid > 1024) *grid = 1024;
+    return cudaSuccess;
+  });
 }
 
 template <int KIND, int PASS, bool C64>
@@ -2046,21 +2045,23 @@ template <bool P2>
 static cudaError_t launch_select_t(OpArgs a, int ns, int kind, int gh, int mode, int j, int trace,
                                    cudaStream_t s) {
   const size_t smem = kSelSmem;
-  static int grid = 0;
-  if (grid == 0) {
+  static PerDevice cache;
+  int grid = 0;
+  cudaError_t e = per_device(cache, &grid, [smem](int* g) {
     const void* f = (const void*)k_select_coop<P2>;
-    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    cudaError_t e2 = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e2 != cudaSuccess) return e2;
     int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kSelThreads, smem);
-    if (e != cudaSuccess) return e;
+    e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kSelThreads, smem);
+    if (e2 != cudaSuccess) return e2;
     if (occ < 1) return cudaErrorInvalidConfiguration;
-    grid = device().sms * occ;
-    if (grid > 1024) grid = 1024;  // per-CTA partials
-  }
+    *g = device().sms * occ;
+    if (*g > 1024) *g = 1024;  // per-CTA partials
+    return cudaSuccess;
+  });
+  if (e != cudaSuccess) return e;
   a.prof = prof_on() ? 1 : 0;
   dim3 grd(grid), blk(kSelThreads);
-  cudaError_t e = cudaSuccess;
   KLAUNCH(S_SELECT1, s, e = launch_coop(k_select_coop<P2>, grd, blk, smem, s, a, ns, kind, gh, mode, j, trace));
   return e;
 }
@@ -2362,6 +2363,30 @@ static int seg_grid(F kern, int threads, size_t smem, int nseg) {
   return g > nseg ? g : nseg;
 }
 
+// The resident grid of the segmented selection on the current device (one
+// block group per segment, so a launch takes at most this many segments).
+template <bool P2>
+static cudaError_t seg_select_grid(int* out) {
+  static PerDevice cache;
+  return per_device(cache, out, [](int* g) {
+    const size_t ssmem = kSelSmem;
+    cudaError_t e = cudaFuncSetAttribute(k_select_seg<P2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem);
+    if (e != cudaSuccess) return e;
+    *g = seg_grid(k_select_seg<P2>, kSelThreads, ssmem, 1);
+    if (*g > 1024) *g = 1024;
+    return cudaSuccess;
+  });
+}
+
+cudaError_t seg_max_segments(int* out) {
+  int a = 0, b = 0;
+  cudaError_t e = seg_select_grid<true>(&a);
+  if (e == cudaSuccess) e = seg_select_grid<false>(&b);
+  if (e != cudaSuccess) return e;
+  *out = a < b ? a : b;
+  return cudaSuccess;
+}
+
 template <int KIND, bool C64>
 static cudaError_t merge_op_seg(const OpArgs* ops, int nseg, int fin_mode, int trace, SegPlan* plan,
                                 cudaStream_t s) {
@@ -2384,26 +2409,14 @@ static cudaError_t merge_op_seg(const OpArgs* ops, int nseg, int fin_mode, int t
   const size_t ssmem = kSelSmem;
   cudaError_t e = cudaSuccess;
   if (fin_mode == 1) {
-    static int gs1 = 0;
-    if (gs1 == 0) {
-      if ((e = cudaFuncSetAttribute(k_select_seg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem)) !=
-          cudaSuccess)
-        return e;
-      gs1 = seg_grid(k_select_seg<true>, kSelThreads, ssmem, 1);
-      if (gs1 > 1024) gs1 = 1024;
-    }
+    int gs1 = 0;
+    if ((e = seg_select_grid<true>(&gs1)) != cudaSuccess) return e;
     if (nseg > gs1) return cudaErrorInvalidValue;  // the groups' barriers need every block resident
     KLAUNCH(S_SELECT1, s, e = launch_coop(k_select_seg<true>, dim3(gs1), dim3(kSelThreads), ssmem, s, ops, plan, ns,
                                           (int)KIND, gt, fin_mode, trace));
   } else {
-    static int gs0 = 0;
-    if (gs0 == 0) {
-      if ((e = cudaFuncSetAttribute(k_select_seg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem)) !=
-          cudaSuccess)
-        return e;
-      gs0 = seg_grid(k_select_seg<false>, kSelThreads, ssmem, 1);
-      if (gs0 > 1024) gs0 = 1024;
-    }
+    int gs0 = 0;
+    if ((e = seg_select_grid<false>(&gs0)) != cudaSuccess) return e;
     if (nseg > gs0) return cudaErrorInvalidValue;
     KLAUNCH(S_SELECT1, s, e = launch_coop(k_select_seg<false>, dim3(gs0), dim3(kSelThreads), ssmem, s, ops, plan, ns,
                                           (int)KIND, gt, fin_mode, trace));

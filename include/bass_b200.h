@@ -325,6 +325,10 @@ typedef struct bass_seg_op {
   int32_t pad;
 } bass_seg_op;
 size_t bass_batch_ws_bytes(int max_ops);
+/* The most states one segmented call takes on the current device (a call's
+   selection keeps one block group per state resident; no counterpart in the
+   reference, which has no batched path).  0 if no device. */
+int bass_batch_max_segments(void);
 /* bass_gate_1q on every segment (sparse_state.py:15-67 + truncation) */
 int bass_gate_1q_batch(const bass_seg_op* host_ops, int n, void* batch_ws, size_t batch_ws_bytes, void* stream);
 /* bass_gate_2q on every segment (bass_simulator.py:292-354 + truncation) */
