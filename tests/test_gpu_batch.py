@@ -105,6 +105,24 @@ def test_batch_c64_equals_plain_c64(env):
         assert p.gamma == st.gamma
 
 
+def test_batch_more_circuits_than_one_launch_takes(env):
+    # more live circuits than one segmented launch takes (one selection block
+    # per SM): every stage splits its ops over several launches
+    from bass_b200 import _native
+    from bass_b200.bass import BASS
+    from bass_b200.batch import BatchedBASS
+    limit = int(_native.lib().bass_batch_max_segments())
+    assert limit >= 1
+    count = min(limit + 40, 250)
+    specs, circs = env.circuits.config4_batch(seed=9, count=count, n_range=(6, 10), layer_range=(2, 4),
+                                              m_range=(3, 5), dt=0.3, disorder_h=0.25)
+    got = BatchedBASS(specs, dtype=np.complex128).simulate(circs)
+    for i in (0, limit - 1, limit, count - 1):
+        st = BASS(*specs[i]).simulate(circs[i])
+        assert np.array_equal(st.x, got[i].x) and np.array_equal(st.alpha, got[i].alpha)
+        assert st.gamma == got[i].gamma
+
+
 def test_batch_result_same_alone_and_in_mix(env):
     from bass_b200.batch import BatchedBASS
     specs, circs = _mix(env)
