@@ -51,6 +51,48 @@ __device__ __forceinline__ long long wait_limit(const bass_ctrl* c) {
 }
 
 // ---------------------------------------------------------------------------
+// bulk asynchronous copies (TMA, untiled) into this CTA's shared memory
+// ---------------------------------------------------------------------------
+// Global source and shared destination 16-byte aligned, sizes multiples of
+// 16 bytes; the source is always this GPU's own memory and no copy is
+// multicast.  Completion is counted in bytes on an mbarrier of the CTA.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned arrivals) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n\tfence.mbarrier_init.release.cluster;" ::"r"(
+                   smem_addr(bar)),
+               "r"(arrivals)
+               : "memory");
+}
+// One arrival that also expects `bytes` of copies on the current phase.
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// true once the phase of the given parity has completed (the thread may be
+// suspended for up to about a microsecond before it returns false)
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(1000)
+      : "memory");
+  return ok != 0;
+}
+// Orders this CTA's earlier generic-proxy accesses of shared memory (after a
+// barrier: every thread's) before the bulk copies issued next.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// A hint: bring [src, src + bytes) into L2 (no completion to wait for).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
+// ---------------------------------------------------------------------------
 // exact accumulation
 // ---------------------------------------------------------------------------
 // fx_from(v) = trunc(|v| * 2^96) with the sign of v (terms below 2^-96 vanish).

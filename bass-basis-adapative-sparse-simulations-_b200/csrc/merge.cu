@@ -512,6 +512,8 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
   __shared__ SelState S;
   __shared__ long long sItem, sBase, sZstart;
   __shared__ long long sSegLo[5], sSegOff[6];
+  __shared__ int sSegPos[5], sGap[5];
+  __shared__ uint64_t sBar;  // completion of the tile's bulk copies
   __shared__ int sWarp[32];
   __shared__ i128 sRed[4 * (kThreads / 32)];
 
@@ -534,9 +536,15 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
     if (H.c64 != (int)C64) set_error(a.ctrl, BASS_ERR_ARG);  // launched for the other amplitude type
     H.t = (KIND == K_IDENT || KIND == K_RDM) ? 0 : in->pos[a.q];
     H.ntiles = (KIND == K_IDENT) ? plain_tiles(H.n) : merge_tiles(H.n);
+    mbar_init(&sBar, 1);
   }
   out_order_par(a.in, KIND, a.q, a.gb, H.qat_out);
   __syncthreads();
+  // bulk copies need 16-byte aligned arrays (every allocation of this library
+  // is; a caller's arrays at an 8-byte offset take the per-entry copies)
+  const bool tma = ((reinterpret_cast<uintptr_t>(H.keys) | reinterpret_cast<uintptr_t>(H.amps)) & 15) == 0;
+  constexpr unsigned kAmpBytes = C64 ? 8u : 16u;
+  unsigned phase = 0;  // parity of sBar's current phase
 
   const int gb = a.gb;
   const long long ntiles = H.ntiles;
@@ -601,14 +609,79 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
       }
       sSegOff[5] = o;
       sZstart = zs;
+      // shared positions: segment k starts at its packed offset, or one
+      // position later, so that its positions have the parity of its source
+      // entries (both ends of a bulk copy of 8-byte data 16-byte aligned); at
+      // most five gaps, inside kTilePad.  A plain tile has one segment from
+      // an even entry (tile * kTile) and no gap.
+      int gap = 0;
+      for (int k = 0; k < 5; ++k) {
+        const long long ln = sSegOff[k + 1] - sSegOff[k];
+        if (tma && ln > 0 && ((sSegOff[k] + gap - sSegLo[k]) & 1)) ++gap;
+        sGap[k] = gap;
+        sSegPos[k] = (int)sSegOff[k] + gap;
+      }
+      if (tma) {
+        // the bulk copies of every segment's 16-byte aligned body [f, l):
+        // one arrival that expects all their bytes, then the copies
+        unsigned bytes = 0;
+        for (int k = 0; k < 5; ++k) {
+          const long long l0 = sSegLo[k], ln = sSegOff[k + 1] - sSegOff[k];
+          if (ln > 0) bytes += (unsigned)(((l0 + ln) & ~1LL) - ((l0 + 1) & ~1LL)) * (8u + kAmpBytes);
+        }
+        fence_proxy_async_smem();  // the previous tile's shared accesses (all threads: barrier above)
+        mbar_arrive_expect(&sBar, bytes);
+        for (int k = 0; k < 5; ++k) {
+          const long long l0 = sSegLo[k], ln = sSegOff[k + 1] - sSegOff[k];
+          if (ln <= 0) continue;
+          const long long f = (l0 + 1) & ~1LL, l = (l0 + ln) & ~1LL;
+          if (l <= f) continue;
+          const int p = sSegPos[k] + (int)(f - l0);
+          const unsigned nb = (unsigned)(l - f);
+          bulk_load(sZ + p, H.keys + f, 8u * nb, &sBar);
+          if (C64)
+            bulk_load(reinterpret_cast<float2*>(sA) + p, reinterpret_cast<const float2*>(H.amps) + f, 8u * nb, &sBar);
+          else
+            bulk_load(sA + p, H.amps + f, 16u * nb, &sBar);
+        }
+      }
       if (a.prof) atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_in[KIND * 5 + PASS]),
                             (unsigned long long)o);
     }
     __syncthreads();
     const int E = (int)sSegOff[5];
 
-    // ---- load: asynchronous copies straight into shared memory -------------
-    {
+    // ---- load: bulk copies straight into shared memory ------------------------
+    // (issued by thread 0 above); warp 0 fetches the at most two ragged
+    // entries of each segment (an odd first entry, an even last one) with
+    // plain loads, then every thread waits for the copies' bytes on sBar.  The
+    // wait is bounded (the copies complete unless the byte count is wrong);
+    // giving up records BASS_ERR_WAIT and ends the pass.
+    if (tma) {
+      if (tid < 10) {
+        const int k = tid >> 1;
+        const long long l0 = sSegLo[k], ln = sSegOff[k + 1] - sSegOff[k];
+        if (ln > 0) {
+          const long long f = (l0 + 1) & ~1LL, l = (l0 + ln) & ~1LL;
+          const bool last = tid & 1;
+          if (last ? l < l0 + ln : l0 < f) {
+            const long long i = last ? l : l0;
+            const int p = sSegPos[k] + (int)(i - l0);
+            sZ[p] = H.keys[i];
+            if (C64) reinterpret_cast<float2*>(sA)[p] = reinterpret_cast<const float2*>(H.amps)[i];
+            else sA[p] = H.amps[i];
+          }
+        }
+      }
+      bool done = false;
+      for (long long sp = 0; sp < kSpinLimit && !done; ++sp) done = mbar_try_wait(&sBar, phase);
+      phase ^= 1u;
+      if (__syncthreads_or(!done)) {
+        if (tid == 0) set_error(a.ctrl, BASS_ERR_WAIT);
+        break;
+      }
+    } else {
+      // 8-byte aligned arrays: asynchronous per-entry copies (no gaps)
       const int o1 = (int)sSegOff[1], o2 = (int)sSegOff[2], o3 = (int)sSegOff[3], o4 = (int)sSegOff[4];
       const unsigned zb = (unsigned)__cvta_generic_to_shared(sZ);
       const unsigned ab = (unsigned)__cvta_generic_to_shared(sA);
@@ -630,8 +703,8 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
         }
       }
       asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+      __syncthreads();
     }
-    __syncthreads();
 
     // ---- Z order: stable split by the target bit, merge, write back --------
     // The split rewrites the Z keys (zmove of the loaded keys) in place, bit-
@@ -643,11 +716,14 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
       const unsigned lt = (1u << lane) - 1;
       unsigned m0[kPerThread];
       uint64_t zk[kPerThread];
+      int pe[kPerThread];  // shared position of load position e
       int c0 = 0;
+      const int o1 = (int)sSegOff[1], o2 = (int)sSegOff[2], o3 = (int)sSegOff[3], o4 = (int)sSegOff[4];
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
         const int e = w * 256 + k * 32 + lane;
-        zk[k] = e < E ? zmove(sZ[e], t, gb) : ~0ULL;
+        pe[k] = e + sGap[(e >= o1) + (e >= o2) + (e >= o3) + (e >= o4)];
+        zk[k] = e < E ? zmove(sZ[pe[k]], t, gb) : ~0ULL;
         const bool is0 = e < E && !((zk[k] >> gb) & 1ULL);
         m0[k] = __ballot_sync(0xffffffffu, is0);
         c0 += __popc(m0[k]);
@@ -670,7 +746,7 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
         if (e < E) {
           const int dst = ((m0[k] >> lane) & 1u) ? r0 + __popc(m0[k] & lt) : n0 + r1 + __popc(ones & lt);
           sZ[dst] = zk[k];  // in place: every thread read its keys before the barrier above
-          sIdx[dst] = (uint16_t)e;
+          sIdx[dst] = (uint16_t)pe[k];
         }
         r0 += __popc(m0[k]);
         r1 += __popc(ones);
