@@ -1866,33 +1866,84 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
 // One CTA per tile (block-strided).  The tile's children sit at its slot
 // range [NS * P'_b, NS * P'_{b+1}) of the staging arrays, in output order; the
 // survivors (decided by the slot alone, see slot_kept) are written from the
-// tile's base (the selection's scan of the tile counts) on, eight consecutive
-// slots per thread and round.  The last CTA to finish writes the output
-// descriptor.  A rejected rotation candidate is not written.
+// tile's base (the selection's scan of the tile counts) on.  The range is
+// taken in chunks of kChunk slots: thread 0 copies the chunk's slots, staged
+// amplitudes and staged keys into shared memory with TMA bulk copies (their
+// 16-byte aligned bodies; warp 0 fetches the at most two ragged end entries of
+// each array with plain loads), then every thread ranks eight consecutive
+// slots' survivors and writes them from there.  The last CTA to finish writes
+// the output descriptor.  A rejected rotation candidate is not written.
+constexpr int kChunk = 8 * kThreads;  // slots per chunk (one round of eight per thread)
+constexpr int kChunkPad = kChunk + 2;  // an odd first entry sits one position in
+// dynamic shared memory of the compaction: slots, amplitudes (16 B), keys
+constexpr size_t kCompactSmem = (size_t)kChunkPad * (8 + 16 + 8);
+
+// Bulk copy of entries [lo, hi) of an array of `esz`-byte entries (esz 8 or
+// 16) into shared memory at position (index - (lo & ~1)), so that both ends
+// are 16-byte aligned (body_bytes: the bytes it copies).  For 8-byte entries
+// the ragged entries lo (odd) and hi - 1 (even) are left to copy_ragged.
+__device__ __forceinline__ unsigned body_bytes(long long lo, long long hi, unsigned esz) {
+  const long long f = esz == 16 ? lo : (lo + 1) & ~1LL;
+  const long long l = esz == 16 ? hi : hi & ~1LL;
+  return (hi <= lo || l <= f) ? 0u : (unsigned)(esz * (l - f));
+}
+__device__ __forceinline__ void copy_body(void* dst, const void* src, long long lo, long long hi, unsigned esz,
+                                          uint64_t* bar) {
+  const unsigned nb = body_bytes(lo, hi, esz);
+  if (nb == 0) return;
+  const long long f = esz == 16 ? lo : (lo + 1) & ~1LL;
+  const long long e0 = lo & ~1LL;
+  bulk_load(static_cast<unsigned char*>(dst) + esz * (f - e0), static_cast<const unsigned char*>(src) + esz * f, nb,
+            bar);
+}
+// The entry of [lo, hi) that copy_body leaves out at its start (last = false)
+// or end (last = true), if any, by a plain load.
+template <typename E>
+__device__ __forceinline__ void copy_ragged(E* dst, const E* src, long long lo, long long hi, bool last) {
+  if (sizeof(E) == 16 || hi <= lo) return;
+  const long long f = (lo + 1) & ~1LL, l = hi & ~1LL, e0 = lo & ~1LL;
+  if (last ? l < hi : lo < f) {
+    const long long i = last ? l : lo;
+    dst[i - e0] = src[i];
+  }
+}
+
 template <bool C64>
 __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int kind) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long* cS = reinterpret_cast<unsigned long long*>(smem);          // slots
+  double2* cA = reinterpret_cast<double2*>(cS + kChunkPad);                        // amplitudes
+  float2* cAf = reinterpret_cast<float2*>(cA);
+  uint64_t* cK = reinterpret_cast<uint64_t*>(cA + kChunkPad);                      // staged keys
   __shared__ SelState S;
   __shared__ int sCnt[8][kThreads / 32];  // survivors per (round u, warp)
+  __shared__ uint64_t sBar;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   load_sel(&S, a.ws.sel);
+  if (tid == 0) mbar_init(&sBar, 1);
   __syncthreads();
   const long long n = a.in->nnz;
   const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
-  const bool ok = ntiles <= a.ws.max_tiles && (long long)ns * n <= a.ws.max_n;
+  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
+  const bool aligned = ((reinterpret_cast<uintptr_t>(slots) | reinterpret_cast<uintptr_t>(a.ws.tmp_amps) |
+                         reinterpret_cast<uintptr_t>(a.ws.stage_keys)) & 15) == 0;
+  const bool ok = ntiles <= a.ws.max_tiles && (long long)ns * n <= a.ws.max_n && aligned;
   if (!ok && g.bid == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
   const unsigned long long T = S.do_trunc ? S.t_bits : 0ULL;
   const bool incl = !S.do_trunc || S.t_key == ~0ULL;
-  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
   uint64_t* okeys = a.out->keys;
   double2* oamps = reinterpret_cast<double2*>(a.out->amps);
   float2* oampf = reinterpret_cast<float2*>(a.out->amps);
   const float2* stf = reinterpret_cast<const float2*>(a.ws.tmp_amps);
   constexpr bool c64 = C64;
+  constexpr unsigned kAmpBytes = C64 ? 8u : 16u;
   const long long cap = a.out->cap;
   const int lns = ns == 4 ? 2 : ns == 2 ? 1 : 0;
   const unsigned lt = (1u << lane) - 1;
   long long written = 0;
-  for (long long b = g.bid; ok && !S.skip_write && b < ntiles; b += g.nblk) {
+  unsigned phase = 0;
+  bool stop = !ok || S.skip_write;
+  for (long long b = g.bid; !stop && b < ntiles; b += g.nblk) {
     long long z0, z1;
     if (kind == K_IDENT) {
       z0 = b * kTile;
@@ -1903,19 +1954,45 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
     }
     const long long s1 = ns * z1;
     long long base = (long long)a.ws.status[b];
-    // rounds of 8 x 256 slots; slot (u, tid) = i0 + 256 u + tid, so every
-    // warp load and store covers consecutive slots
-    for (long long i0 = ns * z0; i0 < s1; i0 += 8 * kThreads) {
-      // all loads of the round first, then the ranks, then the stores
+    // chunks of 8 x 256 slots; slot (u, tid) = i0 + 256 u + tid, so every
+    // warp's shared reads and global stores cover consecutive slots
+    for (long long i0 = ns * z0; i0 < s1; i0 += kChunk) {
+      const long long i1 = (i0 + kChunk < s1) ? i0 + kChunk : s1;
+      const long long q0 = i0 >> lns, q1 = ((i1 - 1) >> lns) + 1;  // staged keys of the chunk
+      const long long e0 = i0 & ~1LL, k0 = q0 & ~1LL;
+      if (tid == 0) {
+        fence_proxy_async_smem();  // the previous chunk's shared accesses (barrier at its end)
+        // the expected bytes first (one arrival), then the copies
+        mbar_arrive_expect(&sBar, body_bytes(i0, i1, 8) + body_bytes(i0, i1, kAmpBytes) + body_bytes(q0, q1, 8));
+        copy_body(cS, slots, i0, i1, 8, &sBar);
+        if (C64) copy_body(cAf, stf, i0, i1, 8, &sBar);
+        else copy_body(cA, a.ws.tmp_amps, i0, i1, 16, &sBar);
+        copy_body(cK, a.ws.stage_keys, q0, q1, 8, &sBar);
+      }
+      if (tid < 6) {
+        const bool last = tid & 1;
+        if (tid < 2) copy_ragged(cS, slots, i0, i1, last);
+        else if (tid < 4) {
+          if (C64) copy_ragged(cAf, stf, i0, i1, last);
+        } else {
+          copy_ragged(cK, a.ws.stage_keys, q0, q1, last);
+        }
+      }
+      bool done = false;
+      for (long long sp = 0; sp < kSpinLimit && !done; ++sp) done = mbar_try_wait(&sBar, phase);
+      phase ^= 1u;
+      if (__syncthreads_or(!done)) {
+        if (tid == 0) set_error(a.ctrl, BASS_ERR_WAIT);
+        stop = true;
+        break;
+      }
       unsigned long long x[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const long long i = i0 + u * kThreads + tid;
-        x[u] = (i < s1) ? __ldcs(slots + i) : ~0ULL;
+        x[u] = (i < i1) ? cS[i - e0] : ~0ULL;
       }
       unsigned bal[8];
-      unsigned long long kk[8];
-      double2 aa[8];
       unsigned km = 0, tm = 0;
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
@@ -1925,23 +2002,13 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
       // children tied at the threshold pattern: kept up to the true key t_key
       for (unsigned r = tm; r; r &= r - 1) {
         const int u = __ffs(r) - 1;
-        if (true_key(staged_key(a.ws.stage_keys, i0 + u * kThreads + tid, lns, true), S.qat, 64) <= S.t_key)
-          km |= 1u << u;
+        const long long i = i0 + u * kThreads + tid;
+        const uint64_t key = cK[(i >> lns) - k0] | (uint64_t)(i & ((1LL << lns) - 1));
+        if (true_key(key, S.qat, 64) <= S.t_key) km |= 1u << u;
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
-        const long long i = i0 + u * kThreads + tid;
-        const bool kept = (km >> u) & 1u;
-        bal[u] = __ballot_sync(0xffffffffu, kept);
-        if (kept) {
-          kk[u] = staged_key(a.ws.stage_keys, i, lns, true);
-          if (c64) {
-            const float2 f = __ldcs(stf + i);
-            aa[u] = make_double2(f.x, f.y);
-          } else {
-            aa[u] = __ldcs(a.ws.tmp_amps + i);
-          }
-        }
+        bal[u] = __ballot_sync(0xffffffffu, (km >> u) & 1u);
         if (lane == 0) sCnt[u][w] = __popc(bal[u]);
       }
       __syncthreads();
@@ -1956,17 +2023,18 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
         const int y = __shfl_up_sync(0xffffffffu, inc, off);
         if (lane >= off) inc += y;
       }
-      const int tot = __shfl_sync(0xffffffffu, inc, 31);  // survivors of the round
+      const int tot = __shfl_sync(0xffffffffu, inc, 31);  // survivors of the chunk
       const int mine = (w & 1) ? inc - c1 : inc - c0 - c1;  // offset of entry 2l + (w & 1)
       if (base + tot <= cap) {
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
           const int ahead = __shfl_sync(0xffffffffu, mine, u * 4 + (w >> 1));  // entry 8u + w
           if ((bal[u] >> lane) & 1u) {
+            const long long i = i0 + u * kThreads + tid;
             const long long o = base + ahead + __popc(bal[u] & lt);
-            okeys[o] = kk[u];
-            if (c64) oampf[o] = make_float2((float)aa[u].x, (float)aa[u].y);  // float values: exact
-            else oamps[o] = aa[u];
+            okeys[o] = cK[(i >> lns) - k0] | (uint64_t)(i & ((1LL << lns) - 1));
+            if (c64) oampf[o] = cAf[i - e0];
+            else oamps[o] = cA[i - e0];
           }
         }
       } else if (tid == 0) {
@@ -1974,7 +2042,7 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
       }
       base += tot;
       written += tot;
-      __syncthreads();  // sCnt is reused by the next round
+      __syncthreads();  // sCnt and the chunk buffers are reused by the next chunk
     }
   }
   if (tid == 0 && a.prof && written)
@@ -2147,6 +2215,21 @@ static cudaError_t launch_select(OpArgs a, int ns, int kind, int gh, int mode, i
                    : launch_select_t<false>(a, ns, kind, gh, mode, j, trace, s);
 }
 
+// Opts a kernel of kThreads threads in to `smem` bytes of dynamic shared
+// memory and returns its resident grid (once per device).
+template <typename K>
+static cudaError_t smem_grid(PerDevice& cache, K kern, size_t smem, int* grid) {
+  return per_device(cache, grid, [kern, smem](int* v) {
+    cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    *v = device().sms * (occ > 0 ? occ : 1);
+    return cudaSuccess;
+  });
+}
+
 template <int KIND>
 static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j, cudaStream_t s) {
   cudaError_t e = cudaSuccess;
@@ -2174,13 +2257,18 @@ static cudaError_t merge_op(OpArgs a, const bass_trunc& tr, int fin_mode, int j,
     return launch_tile<KIND, P_WRITE>(a, 3, s, nullptr);
   } else {
     a.prof = prof_on() ? 1 : 0;
+    static PerDevice grid_c64, grid_c128;
+    int gc = 0;
+    if ((e = a.c64 ? smem_grid(grid_c64, k_compact<true>, kCompactSmem, &gc)
+                   : smem_grid(grid_c128, k_compact<false>, kCompactSmem, &gc)) != cudaSuccess)
+      return e;
     if (a.c64)
       KLAUNCH(KIND * 5 + P_WRITE, s,
-              launch_pdl(k_compact<true>, dim3(device().sms * 4), dim3(kThreads), 0, s, a,
+              launch_pdl(k_compact<true>, dim3(gc), dim3(kThreads), kCompactSmem, s, a,
                          (int)slots_per_entry(KIND), (int)KIND));
     else
       KLAUNCH(KIND * 5 + P_WRITE, s,
-              launch_pdl(k_compact<false>, dim3(device().sms * 4), dim3(kThreads), 0, s, a,
+              launch_pdl(k_compact<false>, dim3(gc), dim3(kThreads), kCompactSmem, s, a,
                          (int)slots_per_entry(KIND), (int)KIND));
     return cudaGetLastError();
   }
@@ -2498,8 +2586,11 @@ static cudaError_t merge_op_seg(const OpArgs* ops, int nseg, int fin_mode, int t
                                           (int)KIND, gt, fin_mode, trace));
   }
   if (e != cudaSuccess) return e;
-  const int gc = device().sms * 4 > nseg ? device().sms * 4 : nseg;
-  KLAUNCH(KIND * 5 + P_WRITE, s, k_compact_seg<C64><<<gc, kThreads, 0, s>>>(ops, plan, ns, (int)KIND));
+  static PerDevice grid_seg;
+  int gc = 0;
+  if ((e = smem_grid(grid_seg, k_compact_seg<C64>, kCompactSmem, &gc)) != cudaSuccess) return e;
+  if (gc < nseg) gc = nseg;
+  KLAUNCH(KIND * 5 + P_WRITE, s, k_compact_seg<C64><<<gc, kThreads, kCompactSmem, s>>>(ops, plan, ns, (int)KIND));
   return cudaGetLastError();
 }
 
