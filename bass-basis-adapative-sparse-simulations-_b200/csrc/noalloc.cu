@@ -21,9 +21,9 @@
 //     the tile counters are cleared at the start of every call, everything else
 //     is fully rewritten by each call;
 //   * the first call on a device resolves the array's device address
-//     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture begins.  The address is cached for the life
-//     of the process; it is not valid after cudaDeviceReset.
+//     (cudaGetSymbolAddress, with that device current).  The address is
+//     cached for the life of the process; it is not valid after
+//     cudaDeviceReset.
 #include <stddef.h>
 
 #include <mutex>

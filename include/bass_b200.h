@@ -268,9 +268,9 @@ int bass_sparse_dot(const bass_state* st, const double* psi, int nq, double* out
    about 1,052,640 entries) is refused on the device: the call returns
    BASS_OK, ctrl->error gets BASS_ERR_WORKSPACE and rho gets NaN.  All calls
    share the array, so calls that may overlap on the GPU race and must be
-   serialised.  The first call on a device looks up the array's address; make
-   it before any stream capture.  The address is kept for the life of the
-   process: it does not survive cudaDeviceReset.  Allocates nothing. */
+   serialised.  The first call on a device looks up the array's address (a
+   runtime query, cudaGetSymbolAddress); the address is kept for the life of
+   the process: it does not survive cudaDeviceReset.  Allocates nothing. */
 int bass_rdm_1q_noalloc(const bass_state* st, int64_t max_entries, int num_qubits, double* rho,
                         bass_ctrl* ctrl, void* stream);
 /* One coordinate-descent step of bass_simulator.py:755-814: rotate qubit j of
