@@ -342,8 +342,16 @@ class DevState:
         check(eng.L.bass_state_export_typed(self.ptr, ctypes.c_void_p(_ptr(ok)), ctypes.c_void_p(_ptr(oa)),
                                             int(bits), self.amp_type, eng.ws_ptr, eng.ws_bytes, eng.ctrl_ptr,
                                             eng.stream), "bass_state_export")
-        x = ok[:n].cpu().numpy().view(np.uint64).copy()
-        a = oa[:2 * n].cpu().numpy().view(self.np_dtype).copy()
+        # both copies into pinned host memory (torch's caching host allocator),
+        # queued back to back, one synchronisation; the arrays view the pinned
+        # buffers, which stay alive with them
+        hk = torch.empty(max(n, 1), dtype=torch.int64, pin_memory=True)
+        ha = torch.empty(2 * max(n, 1), dtype=oa.dtype, pin_memory=True)
+        hk.copy_(ok, non_blocking=True)
+        ha.copy_(oa, non_blocking=True)
+        torch.cuda.current_stream(eng.device).synchronize()
+        x = hk.numpy()[:n].view(np.uint64)
+        a = ha.numpy()[:2 * n].view(self.np_dtype)
         return x, a
 
     def load(self, x, a):

@@ -81,7 +81,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {
   size_t counters, hist1, hist2, sel, status, fp, red, part, partials, cand_bits, cand_key, tmp_keys,
-      tmp_amps, stage_keys, sort_hist, total;
+      tmp_amps, stage_keys, kmask, sort_hist, total;
   long long max_tiles, sort_tiles;
 };
 
@@ -105,6 +105,7 @@ static Layout layout_for(long long max_n) {
   L.tmp_keys = o; o += align256((size_t)max_n * 8);
   L.tmp_amps = o; o += align256((size_t)max_n * 16);
   L.stage_keys = o; o += align256((size_t)max_n * 8);
+  L.kmask = o; o += align256((size_t)max_n / 8 + 64);
   L.sort_hist = o; o += align256((size_t)256 * L.sort_tiles * 4);
   L.total = o;
   return L;
@@ -137,6 +138,7 @@ bool carve(void* ws, size_t ws_bytes, WsView* v) {
   v->tmp_keys = reinterpret_cast<uint64_t*>(b + L.tmp_keys);
   v->tmp_amps = reinterpret_cast<double2*>(b + L.tmp_amps);
   v->stage_keys = reinterpret_cast<uint64_t*>(b + L.stage_keys);
+  v->kmask = reinterpret_cast<uint8_t*>(b + L.kmask);
   v->sort_hist = reinterpret_cast<unsigned int*>(b + L.sort_hist);
   v->max_n = lo;
   v->max_tiles = L.max_tiles;

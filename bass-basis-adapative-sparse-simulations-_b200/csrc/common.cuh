@@ -615,6 +615,8 @@ struct WsView {
   uint64_t* tmp_keys;            // max_n; gate ops: the slot array (|a|^2 bits per child)
   double2* tmp_amps;             // max_n; gate ops: the staged children's amplitudes
   uint64_t* stage_keys;          // max_n; gate ops: the staged children's keys
+  uint8_t* kmask;                // max_n / 8 + 64: one bit per slot, kept by the selection (bit
+                                 // i & 7 of byte i >> 3; the count pass, then the boundary settle)
   unsigned int* sort_hist;       // radix-sort tile histograms (256 x max_tiles)
   i128* red;                     // 1024 per-CTA reduction partials
   unsigned long long* fp;        // 8 fingerprint accumulators

@@ -1531,8 +1531,11 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
 #pragma unroll
       for (int k = 0; k < 3; ++k) v[k] += fx_join96(dh[k], dl[k]);
     }
-    // survivors per tile
+    // the kept bits of the chunk for the write step (a warp stores 32
+    // consecutive bytes)
     const bool live = c < nchunk;
+    if (live) a.ws.kmask[c] = (uint8_t)km;
+    // survivors per tile
     const long long last = (s0 + 7 < nslots ? s0 + 7 : nslots - 1);
     const long long t0 = live ? tile_of(s0 >> lns, kind, part) : -1;
     const long long t1 = live ? tile_of(last >> lns, kind, part) : -1;
@@ -1598,6 +1601,7 @@ __device__ void settle_boundary(const OpArgs& a, int ns, int kind, unsigned long
     if (bits > tb || (bits == tb && (in_smem ? sb[kCandSmem + k] : cand_true_key(a, i, lns, qat)) <= tk)) {
       atomicAdd(reinterpret_cast<unsigned long long*>(a.ws.status + tile_of((long long)(i >> lns), kind, a.ws.part)),
                 1ULL);
+      atomicOr(reinterpret_cast<unsigned int*>(a.ws.kmask) + (i >> 5), 1u << (i & 31));
       vk[0] += fx_from_pbits(bits);
       if (P2) {
         const double p = __longlong_as_double((long long)bits);
@@ -1866,17 +1870,19 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
 // One CTA per tile (block-strided).  The tile's children sit at its slot
 // range [NS * P'_b, NS * P'_{b+1}) of the staging arrays, in output order; the
 // survivors (decided by the slot alone, see slot_kept) are written from the
-// tile's base (the selection's scan of the tile counts) on.  The range is
-// taken in chunks of kChunk slots: thread 0 copies the chunk's slots, staged
+// tile's base (the selection's scan of the tile counts) on.  Which children
+// survive is read from the selection's kept mask (one bit per slot).  The
+// range is taken in chunks of kChunk slots: thread 0 copies the chunk's staged
 // amplitudes and staged keys into shared memory with TMA bulk copies (their
 // 16-byte aligned bodies; warp 0 fetches the at most two ragged end entries of
-// each array with plain loads), then every thread ranks eight consecutive
-// slots' survivors and writes them from there.  The last CTA to finish writes
-// the output descriptor.  A rejected rotation candidate is not written.
+// each array with plain loads), meanwhile every warp reads the mask words of
+// its slots; then the survivors are ranked and written from shared memory.
+// The last CTA to finish writes the output descriptor.  A rejected rotation
+// candidate is not written.
 constexpr int kChunk = 8 * kThreads;  // slots per chunk (one round of eight per thread)
 constexpr int kChunkPad = kChunk + 2;  // an odd first entry sits one position in
-// dynamic shared memory of the compaction: slots, amplitudes (16 B), keys
-constexpr size_t kCompactSmem = (size_t)kChunkPad * (8 + 16 + 8);
+// dynamic shared memory of the compaction: amplitudes (16 B), keys
+constexpr size_t kCompactSmem = (size_t)kChunkPad * (16 + 8);
 
 // Bulk copy of entries [lo, hi) of an array of `esz`-byte entries (esz 8 or
 // 16) into shared memory at position (index - (lo & ~1)), so that both ends
@@ -1911,8 +1917,7 @@ __device__ __forceinline__ void copy_ragged(E* dst, const E* src, long long lo, 
 template <bool C64>
 __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int kind) {
   extern __shared__ __align__(16) unsigned char smem[];
-  unsigned long long* cS = reinterpret_cast<unsigned long long*>(smem);          // slots
-  double2* cA = reinterpret_cast<double2*>(cS + kChunkPad);                        // amplitudes
+  double2* cA = reinterpret_cast<double2*>(smem);                                  // amplitudes
   float2* cAf = reinterpret_cast<float2*>(cA);
   uint64_t* cK = reinterpret_cast<uint64_t*>(cA + kChunkPad);                      // staged keys
   __shared__ SelState S;
@@ -1924,13 +1929,11 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
   __syncthreads();
   const long long n = a.in->nnz;
   const long long ntiles = (kind == K_IDENT) ? plain_tiles(n) : merge_tiles(n);
-  const unsigned long long* slots = reinterpret_cast<const unsigned long long*>(a.ws.tmp_keys);
-  const bool aligned = ((reinterpret_cast<uintptr_t>(slots) | reinterpret_cast<uintptr_t>(a.ws.tmp_amps) |
-                         reinterpret_cast<uintptr_t>(a.ws.stage_keys)) & 15) == 0;
+  const unsigned int* kmw = reinterpret_cast<const unsigned int*>(a.ws.kmask);  // 32 slots per word
+  const bool aligned = ((reinterpret_cast<uintptr_t>(a.ws.tmp_amps) | reinterpret_cast<uintptr_t>(a.ws.stage_keys) |
+                         reinterpret_cast<uintptr_t>(kmw)) & 15) == 0;
   const bool ok = ntiles <= a.ws.max_tiles && (long long)ns * n <= a.ws.max_n && aligned;
   if (!ok && g.bid == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
-  const unsigned long long T = S.do_trunc ? S.t_bits : 0ULL;
-  const bool incl = !S.do_trunc || S.t_key == ~0ULL;
   uint64_t* okeys = a.out->keys;
   double2* oamps = reinterpret_cast<double2*>(a.out->amps);
   float2* oampf = reinterpret_cast<float2*>(a.out->amps);
@@ -1963,20 +1966,33 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
       if (tid == 0) {
         fence_proxy_async_smem();  // the previous chunk's shared accesses (barrier at its end)
         // the expected bytes first (one arrival), then the copies
-        mbar_arrive_expect(&sBar, body_bytes(i0, i1, 8) + body_bytes(i0, i1, kAmpBytes) + body_bytes(q0, q1, 8));
-        copy_body(cS, slots, i0, i1, 8, &sBar);
+        mbar_arrive_expect(&sBar, body_bytes(i0, i1, kAmpBytes) + body_bytes(q0, q1, 8));
         if (C64) copy_body(cAf, stf, i0, i1, 8, &sBar);
         else copy_body(cA, a.ws.tmp_amps, i0, i1, 16, &sBar);
         copy_body(cK, a.ws.stage_keys, q0, q1, 8, &sBar);
       }
-      if (tid < 6) {
+      if (tid < 4) {
         const bool last = tid & 1;
-        if (tid < 2) copy_ragged(cS, slots, i0, i1, last);
-        else if (tid < 4) {
+        if (tid < 2) {
           if (C64) copy_ragged(cAf, stf, i0, i1, last);
         } else {
           copy_ragged(cK, a.ws.stage_keys, q0, q1, last);
         }
+      }
+      // the kept bits of the warp's 32 slots of each round u (slots i0 + 256 u
+      // + 32 w .. + 31; two mask words, shifted to the warp's first slot, the
+      // slots past the chunk cleared)
+      unsigned bal[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const long long p0 = i0 + u * kThreads + 32 * w;
+        const long long nv = i1 - p0;  // slots of the chunk among the 32
+        unsigned bits = 0;
+        if (nv > 0) {  // p0 < nslots: both words lie inside the mask (nslots / 8 + 64 bytes)
+          const unsigned lo = __ldcg(kmw + (p0 >> 5)), hi = __ldcg(kmw + (p0 >> 5) + 1);
+          bits = __funnelshift_r(lo, hi, (unsigned)(p0 & 31));
+        }
+        bal[u] = nv >= 32 ? bits : (nv <= 0 ? 0u : bits & ((1u << nv) - 1u));
       }
       bool done = false;
       for (long long sp = 0; sp < kSpinLimit && !done; ++sp) done = mbar_try_wait(&sBar, phase);
@@ -1986,31 +2002,9 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
         stop = true;
         break;
       }
-      unsigned long long x[8];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const long long i = i0 + u * kThreads + tid;
-        x[u] = (i < i1) ? cS[i - e0] : ~0ULL;
-      }
-      unsigned bal[8];
-      unsigned km = 0, tm = 0;
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        km |= (unsigned)slot_kept(x[u], T, incl) << u;
-        tm |= (unsigned)(!incl && x[u] == T && x[u] != ~0ULL) << u;
-      }
-      // children tied at the threshold pattern: kept up to the true key t_key
-      for (unsigned r = tm; r; r &= r - 1) {
-        const int u = __ffs(r) - 1;
-        const long long i = i0 + u * kThreads + tid;
-        const uint64_t key = cK[(i >> lns) - k0] | (uint64_t)(i & ((1LL << lns) - 1));
-        if (true_key(key, S.qat, 64) <= S.t_key) km |= 1u << u;
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        bal[u] = __ballot_sync(0xffffffffu, (km >> u) & 1u);
+      for (int u = 0; u < 8; ++u)
         if (lane == 0) sCnt[u][w] = __popc(bal[u]);
-      }
       __syncthreads();
       // the 64 survivor counts in slot order (round major, warp minor): every
       // warp scans them itself, lane l holding entries 2l and 2l + 1
