@@ -1881,8 +1881,9 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
 // candidate is not written.
 constexpr int kChunk = 8 * kThreads;  // slots per chunk (one round of eight per thread)
 constexpr int kChunkPad = kChunk + 2;  // an odd first entry sits one position in
-// dynamic shared memory of the compaction: amplitudes (16 B), keys
-constexpr size_t kCompactSmem = (size_t)kChunkPad * (16 + 8);
+constexpr int kMaskWords = kChunk / 32 + 8;  // the chunk's kept-mask words, from a 16-byte boundary
+// dynamic shared memory of the compaction: amplitudes (16 B), keys, mask words
+constexpr size_t kCompactSmem = (size_t)kChunkPad * (16 + 8) + 4 * kMaskWords;
 
 // Bulk copy of entries [lo, hi) of an array of `esz`-byte entries (esz 8 or
 // 16) into shared memory at position (index - (lo & ~1)), so that both ends
@@ -1920,6 +1921,7 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
   double2* cA = reinterpret_cast<double2*>(smem);                                  // amplitudes
   float2* cAf = reinterpret_cast<float2*>(cA);
   uint64_t* cK = reinterpret_cast<uint64_t*>(cA + kChunkPad);                      // staged keys
+  unsigned int* cM = reinterpret_cast<unsigned int*>(cK + kChunkPad);              // kept-mask words
   __shared__ SelState S;
   __shared__ int sCnt[8][kThreads / 32];  // survivors per (round u, warp)
   __shared__ uint64_t sBar;
@@ -1963,10 +1965,15 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
       const long long i1 = (i0 + kChunk < s1) ? i0 + kChunk : s1;
       const long long q0 = i0 >> lns, q1 = ((i1 - 1) >> lns) + 1;  // staged keys of the chunk
       const long long e0 = i0 & ~1LL, k0 = q0 & ~1LL;
+      // mask words [m0, m1): every word of the chunk's slots and the one after
+      // (the funnel shift's high word), widened to 16-byte boundaries; inside
+      // the mask's nslots / 8 + 64 bytes
+      const long long m0 = (i0 >> 5) & ~3LL, m1 = ((((i1 - 1) >> 5) + 2) + 3) & ~3LL;
       if (tid == 0) {
         fence_proxy_async_smem();  // the previous chunk's shared accesses (barrier at its end)
         // the expected bytes first (one arrival), then the copies
-        mbar_arrive_expect(&sBar, body_bytes(i0, i1, kAmpBytes) + body_bytes(q0, q1, 8));
+        mbar_arrive_expect(&sBar, body_bytes(i0, i1, kAmpBytes) + body_bytes(q0, q1, 8) + 4u * (unsigned)(m1 - m0));
+        bulk_load(cM, kmw + m0, 4u * (unsigned)(m1 - m0), &sBar);
         if (C64) copy_body(cAf, stf, i0, i1, 8, &sBar);
         else copy_body(cA, a.ws.tmp_amps, i0, i1, 16, &sBar);
         copy_body(cK, a.ws.stage_keys, q0, q1, 8, &sBar);
@@ -1979,6 +1986,14 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
           copy_ragged(cK, a.ws.stage_keys, q0, q1, last);
         }
       }
+      bool done = false;
+      for (long long sp = 0; sp < kSpinLimit && !done; ++sp) done = mbar_try_wait(&sBar, phase);
+      phase ^= 1u;
+      if (__syncthreads_or(!done)) {
+        if (tid == 0) set_error(a.ctrl, BASS_ERR_WAIT);
+        stop = true;
+        break;
+      }
       // the kept bits of the warp's 32 slots of each round u (slots i0 + 256 u
       // + 32 w .. + 31; two mask words, shifted to the warp's first slot, the
       // slots past the chunk cleared)
@@ -1988,19 +2003,11 @@ __device__ __forceinline__ void compact_body(const OpArgs& a, Grp g, int ns, int
         const long long p0 = i0 + u * kThreads + 32 * w;
         const long long nv = i1 - p0;  // slots of the chunk among the 32
         unsigned bits = 0;
-        if (nv > 0) {  // p0 < nslots: both words lie inside the mask (nslots / 8 + 64 bytes)
-          const unsigned lo = __ldcg(kmw + (p0 >> 5)), hi = __ldcg(kmw + (p0 >> 5) + 1);
-          bits = __funnelshift_r(lo, hi, (unsigned)(p0 & 31));
+        if (nv > 0) {
+          const int mw = (int)((p0 >> 5) - m0);
+          bits = __funnelshift_r(cM[mw], cM[mw + 1], (unsigned)(p0 & 31));
         }
         bal[u] = nv >= 32 ? bits : (nv <= 0 ? 0u : bits & ((1u << nv) - 1u));
-      }
-      bool done = false;
-      for (long long sp = 0; sp < kSpinLimit && !done; ++sp) done = mbar_try_wait(&sBar, phase);
-      phase ^= 1u;
-      if (__syncthreads_or(!done)) {
-        if (tid == 0) set_error(a.ctrl, BASS_ERR_WAIT);
-        stop = true;
-        break;
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u)
