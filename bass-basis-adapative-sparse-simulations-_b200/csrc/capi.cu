@@ -194,12 +194,19 @@ size_t bass_workspace_bytes(int64_t max_in, int64_t max_out, int num_qubits) {
 }
 
 static bool amp_type_ok(int t) { return t == BASS_AMP_C128 || t == BASS_AMP_C64; }
+// Key arrays are read as 8-byte words, amplitude arrays as 16-byte
+// (complex128) or 8-byte (complex64) vectors.
+static bool arrays_aligned(const void* keys, const void* amps, int amp_type) {
+  const uintptr_t ka = reinterpret_cast<uintptr_t>(keys), aa = reinterpret_cast<uintptr_t>(amps);
+  return (ka & 7) == 0 && (aa & (amp_type == BASS_AMP_C64 ? 7 : 15)) == 0;
+}
 
 int bass_state_init_typed(bass_state* st, uint64_t* keys, double* amps, int64_t cap, int num_qubits,
                           uint64_t init_key, int amp_type, void* stream) {
   if (!st || !keys || !amps || cap < 1 || num_qubits < 1 || num_qubits > BASS_MAX_QUBITS || !amp_type_ok(amp_type))
     return BASS_ERR_ARG;
   if (num_qubits < 64 && (init_key >> num_qubits) != 0) return BASS_ERR_ARG;
+  if (!arrays_aligned(keys, amps, amp_type)) return BASS_ERR_ARG;
   remember_type(st, amp_type);
   return status_of(run_state_init(st, keys, amps, cap, num_qubits, init_key, amp_type, (cudaStream_t)stream));
 }
@@ -214,6 +221,8 @@ int bass_state_import_typed(bass_state* st, uint64_t* st_keys, double* st_amps, 
                             void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
   if (!st || !st_keys || !st_amps || (n > 0 && (!keys || !amps)) || n < 0 || n > cap || num_qubits < 1 ||
       num_qubits > BASS_MAX_QUBITS || !ctrl || !amp_type_ok(amp_type))
+    return BASS_ERR_ARG;
+  if (!arrays_aligned(st_keys, st_amps, amp_type) || (n > 0 && !arrays_aligned(keys, amps, amp_type)))
     return BASS_ERR_ARG;
   CHECK_WS(ws, ws_bytes, v);
   if (n > v.max_n) return BASS_ERR_WORKSPACE;
@@ -233,6 +242,7 @@ int bass_state_export_typed(const bass_state* st, uint64_t* out_keys, double* ou
                             int amp_type, void* ws, size_t ws_bytes, bass_ctrl* ctrl, void* stream) {
   if (!st || !out_keys || !out_amps || !ctrl || key_bits < 1 || key_bits > 64 || !amp_type_ok(amp_type))
     return BASS_ERR_ARG;
+  if (!arrays_aligned(out_keys, out_amps, amp_type)) return BASS_ERR_ARG;
   CHECK_WS(ws, ws_bytes, v);
   return status_of(run_export(st, out_keys, out_amps, key_bits, v, ctrl, (cudaStream_t)stream, amp_type));
 }

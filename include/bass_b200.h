@@ -137,6 +137,11 @@ size_t bass_ctrl_bytes(void);
 size_t bass_workspace_bytes(int64_t max_in, int64_t max_out, int num_qubits);
 
 /* ---- state management ----------------------------------------------------- */
+/* Every key array is 8-byte aligned and every amplitude array 16-byte
+   (complex128) or 8-byte (complex64) aligned, as every cudaMalloc'd or torch
+   buffer is; init, import and export refuse other arrays with BASS_ERR_ARG
+   before touching the GPU.  Tile loads take TMA bulk copies where both arrays
+   of a state are 16-byte aligned, per-entry copies otherwise. */
 /* SparseState.__init__ (sparse_state.py:202-219): |init_key>, amplitude 1. */
 int bass_state_init(bass_state* st, uint64_t* keys, double* amps, int64_t cap, int num_qubits,
                     uint64_t init_key, void* stream);

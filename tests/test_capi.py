@@ -60,6 +60,31 @@ def test_lcg_choose_matches_reference_rule(native, orc):
         assert np.array_equal(idx.astype(np.uint64), xo)
 
 
+def test_state_arrays_must_be_aligned(native):
+    """Keys 8-byte, complex128 amplitudes 16-byte, complex64 amplitudes
+    8-byte aligned: other arrays are refused with BASS_ERR_ARG before any
+    CUDA call (the addresses below are never dereferenced)."""
+    import ctypes
+    L = native.load_library()
+    ERR_ARG, C128, C64 = 3, 0, 1
+    desc = ctypes.create_string_buffer(L.bass_state_bytes())
+    p = ctypes.c_void_p
+    st, ctrl, ws = p(ctypes.addressof(desc)), p(0x7000), p(0x9000)
+    base = 0x100000
+    # init: 8-byte-offset complex128 amplitudes, 4-byte-offset keys
+    assert L.bass_state_init_typed(st, p(base), p(base + 8), 16, 10, 0, C128, None) == ERR_ARG
+    assert L.bass_state_init_typed(st, p(base + 4), p(base + 16), 16, 10, 0, C128, None) == ERR_ARG
+    assert L.bass_state_init_typed(st, p(base + 4), p(base + 8), 16, 10, 0, C64, None) == ERR_ARG
+    assert L.bass_state_init_typed(st, p(base), p(base + 4), 16, 10, 0, C64, None) == ERR_ARG
+    # import: the state's arrays and the input arrays
+    assert L.bass_state_import_typed(st, p(base), p(base + 8), 16, p(base), p(base + 16), 4, 10, C128,
+                                     ws, 1 << 20, ctrl, None) == ERR_ARG
+    assert L.bass_state_import_typed(st, p(base), p(base + 16), 16, p(base + 4), p(base + 16), 4, 10, C128,
+                                     ws, 1 << 20, ctrl, None) == ERR_ARG
+    # export
+    assert L.bass_state_export_typed(st, p(base), p(base + 8), 64, C128, ws, 1 << 20, ctrl, None) == ERR_ARG
+
+
 def test_library_refuses_without_gpu(native):
     import torch
     if torch.cuda.is_available():
