@@ -1424,7 +1424,8 @@ __device__ __forceinline__ long long tile_of(long long z, int kind, const long l
 // A grid-stride stream over the slot array, eight consecutive slots per
 // thread: the survivors per tile (atomically added into ws.status[tile],
 // which the op cleared; one atomic per warp when its 256 slots lie in one
-// tile) and, per CTA in partials s[0..2], the exact mass of the survivors,
+// tile), the kept mask (the thread's eight kept bits as one byte of
+// ws.kmask), and, per CTA in partials s[0..2], the exact mass of the survivors,
 // their sum of |a|^4 (P2) and the exact mass of all children (when
 // truncating).  cand: the children of the level-2 boundary bin (bits >> 37 ==
 // cpre, all below T) are listed as well (slot indices in ws.cand_bits,
@@ -1568,8 +1569,9 @@ __device__ void count_phase(const OpArgs& a, int ns, int kind, unsigned long lon
 // the count pass) are below every kept child of the other bins.  Run by one
 // block (the last to finish): the need-th best of them by (bits desc, true
 // key asc) gives (t_bits, t_key); the kept ones are added to their tiles'
-// counts and to this thread's share of the kept mass (vk[0]) and sum of
-// |a|^4 (vk[1]).  qat: the op's output order (for the true keys).
+// counts, to the kept mask and to this thread's share of the kept mass
+// (vk[0]) and sum of |a|^4 (vk[1]).  qat: the op's output order (for the
+// true keys).
 template <bool P2>
 __device__ void settle_boundary(const OpArgs& a, int ns, int kind, unsigned long long lpre, long long lneed,
                                 const int8_t* qat, i128* vk) {
@@ -1869,14 +1871,14 @@ __global__ void __launch_bounds__(kSelThreads) k_select_coop(const __grid_consta
 // ---------------------------------------------------------------------------
 // One CTA per tile (block-strided).  The tile's children sit at its slot
 // range [NS * P'_b, NS * P'_{b+1}) of the staging arrays, in output order; the
-// survivors (decided by the slot alone, see slot_kept) are written from the
-// tile's base (the selection's scan of the tile counts) on.  Which children
-// survive is read from the selection's kept mask (one bit per slot).  The
-// range is taken in chunks of kChunk slots: thread 0 copies the chunk's staged
-// amplitudes and staged keys into shared memory with TMA bulk copies (their
-// 16-byte aligned bodies; warp 0 fetches the at most two ragged end entries of
-// each array with plain loads), meanwhile every warp reads the mask words of
-// its slots; then the survivors are ranked and written from shared memory.
+// survivors are written from the tile's base (the selection's scan of the
+// tile counts) on.  Which children survive is read from the selection's kept
+// mask (one bit per slot: its count pass and boundary settle).  The range is
+// taken in chunks of kChunk slots: thread 0 copies the chunk's staged
+// amplitudes, staged keys and mask words into shared memory with TMA bulk
+// copies (their 16-byte aligned bodies; warp 0 fetches the at most two ragged
+// 8-byte end entries of each array with plain loads); then the survivors are
+// ranked and written from shared memory.
 // The last CTA to finish writes the output descriptor.  A rejected rotation
 // candidate is not written.
 constexpr int kChunk = 8 * kThreads;  // slots per chunk (one round of eight per thread)
