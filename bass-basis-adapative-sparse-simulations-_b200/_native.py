@@ -67,6 +67,8 @@ SLOT_NAMES[0 * 5 + 3] = "k_compact<gate1>"
 SLOT_NAMES[1 * 5 + 3] = "k_compact<rot1>"
 SLOT_NAMES[2 * 5 + 3] = "k_compact<gate2>"
 SLOT_NAMES[4 * 5 + 3] = "k_compact<plain>"
+# the RDM qubits at low physical bits: one pass of k_rdm_low (the RDM kind's evaluation slot)
+SLOT_NAMES[5 * 5 + 0] = "k_rdm_low"
 
 
 class Trunc(ctypes.Structure):

@@ -36,7 +36,7 @@ struct OpArgs {
   long long k_cond, k_keep;
   bass_trunc tr;  // finalize_op: gamma / renormalisation rules
   int c64;        // the input state stores complex64 amplitudes (selects the kernels)
-  int pad;
+  int rdm_low;    // K_RDM: the qubits at physical bits below kRdmLowBits are left to k_rdm_low
   double* rho;    // RDM moments of a segmented RDM (4 per qubit)
 };
 

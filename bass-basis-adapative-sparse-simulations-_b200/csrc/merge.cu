@@ -95,6 +95,7 @@ __device__ __forceinline__ void partition_body(const OpArgs& a, int kind, int ze
   const long long n = in->nnz;
   const int q = (kind == K_RDM) ? set : a.q;
   const int t = in->pos[q];
+  if (kind == K_RDM && a.rdm_low && t < kRdmLowBits) return;  // paired by k_rdm_low
   const int gb = a.gb;
   const int sh = gb + 1;
   const uint64_t* keys = in->keys;
@@ -557,7 +558,19 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
   // P_RDM: items are (set, tile); K_RDM sets are qubits, the 4x4 moments of
   // a qubit pair (K_GATE2) split into a.nsets = 4 sets of four values that
   // share one partition
-  const long long nitems = (bad || skip) ? 0 : (PASS == P_RDM) ? ntiles * a.nsets : ntiles;
+  // P_RDM of K_RDM with rdm_low: the items cover only the sets whose qubit
+  // sits at physical bit kRdmLowBits or above (sHigh, the same list in every
+  // CTA); k_rdm_low does the others
+  __shared__ int8_t sHigh[64];
+  __shared__ int sNHigh;
+  if (PASS == P_RDM && tid == 0) {
+    int nh = 0;
+    for (int s2 = 0; s2 < a.nsets && s2 < 64; ++s2)
+      if (!(KIND == K_RDM && a.rdm_low && a.in->pos[a.q + s2] < kRdmLowBits)) sHigh[nh++] = (int8_t)s2;
+    sNHigh = nh;
+  }
+  __syncthreads();
+  const long long nitems = (bad || skip) ? 0 : (PASS == P_RDM) ? ntiles * sNHigh : ntiles;
   long long cnt = 0;
   const int base_e = tid * kPerThread;
 
@@ -566,7 +579,7 @@ __device__ __forceinline__ void tile_body(const OpArgs& a, Grp g) {
     __syncthreads();
     const long long item = sItem;
     if (item >= nitems) break;
-    const int set = (PASS == P_RDM) ? (int)(item / ntiles) : 0;
+    const int set = (PASS == P_RDM) ? (int)sHigh[item / ntiles] : 0;
     const long long tile = (PASS == P_RDM) ? item % ntiles : item;
     const int t = (KIND == K_RDM) ? a.in->pos[a.q + set] : H.t;
     const int pset = (KIND == K_RDM) ? set : 0;  // the partition records this item reads
@@ -2062,6 +2075,145 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs 
   compact_body<C64>(a, whole_grid(), ns, kind);
 }
 
+// ---------------------------------------------------------------------------
+// RDM moments of the qubits at low physical bits: one pass
+// ---------------------------------------------------------------------------
+// bass_simulator.py:441-470 for every qubit whose physical bit t is below
+// kRdmLowBits, without a merge pass per qubit: the state is read in plain
+// tiles of kTile entries (key order) plus the next kRdmHalo entries, which
+// hold the partner x | 2^t of every tile entry x with bit t clear (the keys
+// between x and x + 2^t are distinct integers, so at most 2^t - 1 of them
+// come first); a binary search over at most 2^t positions finds it.  The four
+// moments of each such qubit (|a|^2 of its bit-0 and bit-1 entries, re and im
+// of a_x conj(a_{x | 2^t})) are the sums of k_tile's P_RDM pass, exact, into
+// the tile's partials of the qubit's set.
+constexpr int kRdmSpan = kTile + kRdmHalo;
+constexpr int kRdmSpanPad = kRdmSpan + 2;
+constexpr size_t kRdmLowSmem = (size_t)kRdmSpanPad * (16 + 8);  // amplitudes, keys
+
+template <bool C64>
+__global__ void __launch_bounds__(kThreads) k_rdm_low(const __grid_constant__ OpArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* sA = reinterpret_cast<double2*>(smem);
+  float2* sAf = reinterpret_cast<float2*>(sA);
+  uint64_t* sK = reinterpret_cast<uint64_t*>(sA + kRdmSpanPad);
+  __shared__ uint64_t sBar;
+  __shared__ long long sItem;
+  __shared__ i128 sRed[4 * (kThreads / 32)];
+  __shared__ int sSet[kRdmLowBits];  // the set of the qubit at physical bit t, or -1
+  pdl_wait();
+  const int tid = threadIdx.x;
+  const bass_state* in = a.in;
+  const long long n = in->nnz;
+  const long long ntiles = plain_tiles(n);
+  if (tid == 0) mbar_init(&sBar, 1);
+  if (tid < kRdmLowBits) {
+    int set = -1;
+    if (tid < in->nq) {
+      const int q = in->qat[tid] - a.q;
+      if (q >= 0 && q < a.nsets) set = q;
+    }
+    sSet[tid] = set;
+  }
+  const double r0 = in->rscale[0], r1 = in->rscale[1];
+  const bool scaled = !(r0 == 1.0 && r1 == 1.0);
+  const uint64_t* keys = in->keys;
+  const double2* amps = reinterpret_cast<const double2*>(in->amps);
+  const float2* ampf = reinterpret_cast<const float2*>(in->amps);
+  // bulk copies need both arrays 16-byte aligned; keys at an 8-byte offset
+  // take plain loads
+  const bool bulk = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(amps)) & 15) == 0;
+  const bool bad = ntiles > a.ws.max_tiles || (in->amp_type == BASS_AMP_C64) != C64;
+  if (bad && blockIdx.x == 0 && tid == 0) set_error(a.ctrl, BASS_ERR_WORKSPACE);
+  auto amp = [&](int p) {
+    const double2 v = C64 ? f2d(sAf[p]) : sA[p];
+    return scaled ? amp_scale(v, C64 ? 1 : 0, r0, r1) : v;
+  };
+  __syncthreads();
+  unsigned phase = 0;
+  unsigned long long* item_ctr = &reinterpret_cast<unsigned long long*>(a.ws.counters)[a.counter];
+  for (;;) {
+    if (tid == 0) sItem = bad ? ntiles : (long long)atomicAdd(item_ctr, 1ULL);
+    __syncthreads();
+    const long long b = sItem;
+    if (b >= ntiles) break;
+    const long long lo = b * kTile;  // even: both arrays start on 16-byte words
+    const long long own_end = (lo + kTile < n) ? lo + kTile : n;
+    const long long hi = (own_end + kRdmHalo < n) ? own_end + kRdmHalo : n;
+    const int own = (int)(own_end - lo), E = (int)(hi - lo);
+    if (bulk) {
+      if (tid == 0) {
+        fence_proxy_async_smem();  // the previous tile's shared accesses (barrier above)
+        mbar_arrive_expect(&sBar, body_bytes(lo, hi, 8) + body_bytes(lo, hi, C64 ? 8u : 16u));
+        copy_body(sK, keys, lo, hi, 8, &sBar);
+        if (C64) copy_body(sAf, ampf, lo, hi, 8, &sBar);
+        else copy_body(sA, amps, lo, hi, 16, &sBar);
+      }
+      // an odd last entry of the 8-byte arrays (lo is even: no odd first one)
+      if (tid == 0) copy_ragged(sK, keys, lo, hi, true);
+      if (C64 && tid == 1) copy_ragged(sAf, ampf, lo, hi, true);
+      bool done = false;
+      for (long long sp = 0; sp < kSpinLimit && !done; ++sp) done = mbar_try_wait(&sBar, phase);
+      phase ^= 1u;
+      if (__syncthreads_or(!done)) {
+        if (tid == 0) set_error(a.ctrl, BASS_ERR_WAIT);
+        break;
+      }
+    } else {
+      for (int i = tid; i < E; i += kThreads) {
+        sK[i] = keys[lo + i];
+        if (C64) sAf[i] = ampf[lo + i];
+        else sA[i] = amps[lo + i];
+      }
+      __syncthreads();
+    }
+    if (a.prof && tid == 0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&a.ctrl->prof_in[K_RDM * 5 + P_HIST]), (unsigned long long)E);
+    for (int t = 0; t < kRdmLowBits; ++t) {
+      const int set = sSet[t];
+      if (set < 0) continue;  // the same for every thread
+      const uint64_t bit = 1ULL << t;
+      const int reach = 1 << t;  // the partner lies at most this many positions on
+      // at most kPerThread positions per thread: at most eight terms per
+      // split accumulator (fx_acc96) before they are joined
+      i128 v[4] = {0, 0, 0, 0};
+      double dh[4] = {0.0, 0.0, 0.0, 0.0}, dl[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int e = tid; e < own; e += kThreads) {
+        const uint64_t x = sK[e];
+        const double2 ax = amp(e);
+        if (x & bit) {
+          fx_acc96(prob(ax), dh[1], dl[1], v[1]);
+          continue;
+        }
+        fx_acc96(prob(ax), dh[0], dl[0], v[0]);
+        const uint64_t y = x | bit;
+        int L = e + 1;
+        const int R0 = (e + reach < E - 1 ? e + reach : E - 1) + 1;  // search [e + 1, R0)
+        int R = R0;
+        while (L < R) {
+          const int m = (L + R) >> 1;
+          if (sK[m] < y) L = m + 1;
+          else R = m;
+        }
+        if (L < R0 && sK[L] == y) {
+          const double2 ay = amp(L);
+          const double2 c = cmul(ax, make_double2(ay.x, -ay.y));
+          fx_acc96(c.x, dh[2], dl[2], v[2]);
+          fx_acc96(c.y, dh[3], dl[3], v[3]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] += fx_join96s(dh[k], dl[k]);
+      block_sum_i128<4>(v, sRed);
+      if (tid == 0) {
+        Partial* pt = a.ws.partials + (long long)set * a.ws.max_tiles + b;
+        pt->s[0] = v[0]; pt->s[1] = v[1]; pt->s[2] = v[2]; pt->s[3] = v[3];
+      }
+    }
+    __syncthreads();  // the buffers are reused by the next tile
+  }
+}
+
 // Rotation step, after the write pass: keep the candidate if accepted.
 __global__ void k_commit(bass_state* cur, bass_state* tmp, WsView ws, bass_ctrl* c, int j, int trace) {
   const SelState* sel = ws.sel;
@@ -2086,11 +2238,13 @@ __global__ void k_commit(bass_state* cur, bass_state* tmp, WsView ws, bass_ctrl*
   }
 }
 
-__global__ void k_rdm_final(const bass_state* st, double* rho, WsView ws, int first) {
+// low: the sets of qubits at physical bits below kRdmLowBits hold k_rdm_low's
+// partials (one per plain tile), the others the merge pass's (one per merge tile)
+__global__ void k_rdm_final(const bass_state* st, double* rho, WsView ws, int first, int low) {
   __shared__ i128 sRed[4 * 8];
   const int set = blockIdx.x;
   const long long n = st->nnz;
-  const long long ntiles = merge_tiles(n);
+  const long long ntiles = (low && st->pos[first + set] < kRdmLowBits) ? plain_tiles(n) : merge_tiles(n);
   i128 v[4] = {0, 0, 0, 0};
   for (long long t = threadIdx.x; t < ntiles; t += blockDim.x) {
     const Partial& p = ws.partials[(long long)set * ws.max_tiles + t];
@@ -2314,10 +2468,26 @@ cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, 
   a.q = 0;
   a.gb = 0;
   a.nsets = nq;
-  // the partition also clears the small workspace region
+  a.rdm_low = 1;
+  // the partition also clears the small workspace region; the qubits at
+  // physical bits below kRdmLowBits take one pass of k_rdm_low instead of a
+  // partition and a merge pass each
   KLAUNCH(S_PARTITION, s, launch_pdl(k_partition, dim3(device().grid_small, nq), dim3(256), 0, s, a, (int)K_RDM, 1));
   if ((e = launch_tile<K_RDM, P_RDM>(a, 0, s, nullptr)) != cudaSuccess) return e;
-  KLAUNCH(S_RDM_FINAL, s, k_rdm_final<<<nq, 256, 0, s>>>(st, rho, ws, 0));
+  {
+    static PerDevice grid_c64, grid_c128;
+    int gl = 0;
+    if ((e = c64 ? smem_grid(grid_c64, k_rdm_low<true>, kRdmLowSmem, &gl)
+                 : smem_grid(grid_c128, k_rdm_low<false>, kRdmLowSmem, &gl)) != cudaSuccess)
+      return e;
+    a.counter = 5;
+    a.prof = prof_on() ? 1 : 0;
+    if (c64)
+      KLAUNCH(K_RDM * 5 + P_HIST, s, launch_pdl(k_rdm_low<true>, dim3(gl), dim3(kThreads), kRdmLowSmem, s, a));
+    else
+      KLAUNCH(K_RDM * 5 + P_HIST, s, launch_pdl(k_rdm_low<false>, dim3(gl), dim3(kThreads), kRdmLowSmem, s, a));
+  }
+  KLAUNCH(S_RDM_FINAL, s, k_rdm_final<<<nq, 256, 0, s>>>(st, rho, ws, 0, 1));
   return cudaGetLastError();
 }
 
@@ -2339,7 +2509,7 @@ cudaError_t run_rdm_2q(const bass_state* st, bass_state* tmp, int q1, int q2, do
   // the partition also clears the small workspace region
   KLAUNCH(S_PARTITION, s, launch_pdl(k_partition, dim3(device().grid_small, 1), dim3(256), 0, s, b, (int)K_GATE2, 1));
   if ((e = launch_tile<K_GATE2, P_RDM>(b, 0, s, nullptr)) != cudaSuccess) return e;
-  KLAUNCH(S_RDM_FINAL, s, k_rdm_final<<<4, 256, 0, s>>>(tmp, rho, ws, 0));
+  KLAUNCH(S_RDM_FINAL, s, k_rdm_final<<<4, 256, 0, s>>>(tmp, rho, ws, 0, 0));
   return cudaGetLastError();
 }
 
