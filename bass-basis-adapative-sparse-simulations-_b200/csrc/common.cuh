@@ -35,7 +35,7 @@ constexpr int kRankMax = 1024;       // candidates ranked by direct counting (on
 constexpr int kMaxSets = 64;         // partition sets (one per qubit for RDMs)
 // RDM moments of the qubits at physical bits 0 .. kRdmLowBits - 1 come from
 // one pass over plain tiles plus a halo of kRdmHalo entries (k_rdm_low)
-constexpr int kRdmLowBits = 11;
+constexpr int kRdmLowBits = 10;
 constexpr int kRdmHalo = 1 << (kRdmLowBits - 1);
 constexpr int kFxFrac = 96;
 constexpr long long kSpinLimit = 1LL << 22;  // a few seconds at most

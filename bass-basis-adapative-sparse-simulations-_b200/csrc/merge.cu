@@ -2085,8 +2085,10 @@ __global__ void __launch_bounds__(256) k_compact(const __grid_constant__ OpArgs 
 // between x and x + 2^t are distinct integers, so at most 2^t - 1 of them
 // come first); a binary search over at most 2^t positions finds it.  The four
 // moments of each such qubit (|a|^2 of its bit-0 and bit-1 entries, re and im
-// of a_x conj(a_{x | 2^t})) are the sums of k_tile's P_RDM pass, exact, into
-// the tile's partials of the qubit's set.
+// of a_x conj(a_{x | 2^t})) are the sums of k_tile's P_RDM pass, exact:
+// each warp adds its lanes' sums into its own shared accumulators, and at the
+// end every CTA writes one partial per qubit (slot blockIdx.x of the qubit's
+// set; the grid, at most ws.max_tiles, goes to counter 6 for k_rdm_final).
 constexpr int kRdmSpan = kTile + kRdmHalo;
 constexpr int kRdmSpanPad = kRdmSpan + 2;
 constexpr size_t kRdmLowSmem = (size_t)kRdmSpanPad * (16 + 8);  // amplitudes, keys
@@ -2099,10 +2101,11 @@ __global__ void __launch_bounds__(kThreads) k_rdm_low(const __grid_constant__ Op
   uint64_t* sK = reinterpret_cast<uint64_t*>(sA + kRdmSpanPad);
   __shared__ uint64_t sBar;
   __shared__ long long sItem;
-  __shared__ i128 sRed[4 * (kThreads / 32)];
+  __shared__ i128 sAcc[kThreads / 32][kRdmLowBits][4];  // per warp, qubit and moment
   __shared__ int sSet[kRdmLowBits];  // the set of the qubit at physical bit t, or -1
   pdl_wait();
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int i = lane; i < kRdmLowBits * 4; i += 32) sAcc[w][i >> 2][i & 3] = 0;
   const bass_state* in = a.in;
   const long long n = in->nnz;
   const long long ntiles = plain_tiles(n);
@@ -2203,15 +2206,30 @@ __global__ void __launch_bounds__(kThreads) k_rdm_low(const __grid_constant__ Op
         }
       }
 #pragma unroll
-      for (int k = 0; k < 4; ++k) v[k] += fx_join96s(dh[k], dl[k]);
-      block_sum_i128<4>(v, sRed);
-      if (tid == 0) {
-        Partial* pt = a.ws.partials + (long long)set * a.ws.max_tiles + b;
-        pt->s[0] = v[0]; pt->s[1] = v[1]; pt->s[2] = v[2]; pt->s[3] = v[3];
+      for (int k = 0; k < 4; ++k) {
+        v[k] += fx_join96s(dh[k], dl[k]);
+        v[k] = warp_sum_i128(v[k]);
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sAcc[w][t][k] += v[k];
       }
     }
     __syncthreads();  // the buffers are reused by the next tile
   }
+  // the CTA's sums: thread (t, k) adds the warps' accumulators
+  __syncthreads();
+  if (tid < kRdmLowBits * 4) {
+    const int t = tid >> 2, k = tid & 3, set = sSet[t];
+    if (set >= 0 && !bad) {
+      i128 sum = 0;
+#pragma unroll
+      for (int ww = 0; ww < kThreads / 32; ++ww) sum += sAcc[ww][t][k];
+      a.ws.partials[(long long)set * a.ws.max_tiles + blockIdx.x].s[k] = sum;
+    }
+  }
+  if (blockIdx.x == 0 && tid == 0)
+    reinterpret_cast<unsigned long long*>(a.ws.counters)[6] = gridDim.x;
 }
 
 // Rotation step, after the write pass: keep the candidate if accepted.
@@ -2239,12 +2257,15 @@ __global__ void k_commit(bass_state* cur, bass_state* tmp, WsView ws, bass_ctrl*
 }
 
 // low: the sets of qubits at physical bits below kRdmLowBits hold k_rdm_low's
-// partials (one per plain tile), the others the merge pass's (one per merge tile)
+// partials (one per CTA of its grid, counter 6), the others the merge pass's
+// (one per merge tile)
 __global__ void k_rdm_final(const bass_state* st, double* rho, WsView ws, int first, int low) {
   __shared__ i128 sRed[4 * 8];
   const int set = blockIdx.x;
   const long long n = st->nnz;
-  const long long ntiles = (low && st->pos[first + set] < kRdmLowBits) ? plain_tiles(n) : merge_tiles(n);
+  const long long ntiles = (low && st->pos[first + set] < kRdmLowBits)
+                               ? (long long)reinterpret_cast<const unsigned long long*>(ws.counters)[6]
+                               : merge_tiles(n);
   i128 v[4] = {0, 0, 0, 0};
   for (long long t = threadIdx.x; t < ntiles; t += blockDim.x) {
     const Partial& p = ws.partials[(long long)set * ws.max_tiles + t];
@@ -2480,6 +2501,7 @@ cudaError_t run_rdm(const bass_state* st, int nq, double* rho, bass_ctrl* ctrl, 
     if ((e = c64 ? smem_grid(grid_c64, k_rdm_low<true>, kRdmLowSmem, &gl)
                  : smem_grid(grid_c128, k_rdm_low<false>, kRdmLowSmem, &gl)) != cudaSuccess)
       return e;
+    if (gl > ws.max_tiles) gl = (int)ws.max_tiles;  // one partial slot per CTA
     a.counter = 5;
     a.prof = prof_on() ? 1 : 0;
     if (c64)
