@@ -58,8 +58,9 @@ __device__ __forceinline__ long long wait_limit(const bass_ctrl* c) {
 // bulk asynchronous copies (TMA, untiled) into this CTA's shared memory
 // ---------------------------------------------------------------------------
 // Global source and shared destination 16-byte aligned, sizes multiples of
-// 16 bytes; the source is always this GPU's own memory and no copy is
-// multicast.  Completion is counted in bytes on an mbarrier of the CTA.
+// 16 bytes; the source is always this GPU's own memory and every copy lands
+// in the issuing CTA's shared memory only.  Completion is counted in bytes
+// on an mbarrier of the CTA.
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned arrivals) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n\tfence.mbarrier_init.release.cluster;" ::"r"(
